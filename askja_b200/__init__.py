@@ -1,0 +1,406 @@
+"""askja_b200 -- Python mirror of the askja B200 engine's C ABI.
+
+The engine itself is ``libaskja_b200.so`` (CUDA, sm_100a), declared in
+``include/askja_gpu.h``.  This module only binds it with ctypes and mirrors
+the reference's in-process seam under the reference's own names
+(paro8929/askja sun.cpp: ``updateE``, ``updateUandcopyDown``, ``copyDown``,
+``EnergyMag``, ``simpleenergyEl``, ``EnergyEl``, ``TotalEnergy``,
+``GaussLaw``, ``UViol``, ``WilsonLoop``, ``takeconfiguration``,
+``loadconfiguration``, ``initializeU``, ``initializeE``; measurements4d.cpp:
+``PolyakovLoop``, ``WilsonLoop(dir)``, ``PlaqExp``, ``scalarLoopcorr``).
+
+Arrays are numpy complex128 in the reference's U-conf order, shape
+``(V, DIM, NC, NC)`` with the site index x0-slowest.  There is no CPU
+fallback: a missing library or a missing GPU raises ``AskjaError``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libaskja_b200.so")
+EXE_PATH = os.path.join(HERE, "askja")
+
+ASKJA_OK = 0
+ERRORS = {-1: "ASKJA_ERR_ARG", -2: "ASKJA_ERR_CUDA", -3: "ASKJA_ERR_IO", -4: "ASKJA_ERR_NONFINITE",
+          -5: "ASKJA_ERR_NODEVICE", -6: "ASKJA_ERR_PARSE"}
+FP64, FP32 = 0, 1
+MAX_DIM = 16
+
+# every entry point include/askja_gpu.h declares
+EXPORTS = [
+    "askja_create", "askja_destroy", "askja_last_error", "askja_version", "askja_volume", "askja_stream",
+    "askja_sync", "askja_set_links", "askja_get_links", "askja_get_saved_links", "askja_set_momenta",
+    "askja_get_momenta", "askja_initializeU", "askja_hot_start", "askja_initializeE", "askja_updateE",
+    "askja_updateUandcopyDown", "askja_copyDown", "askja_takeconfiguration", "askja_loadconfiguration",
+    "askja_reunitarise", "askja_EnergyMag", "askja_simpleenergyEl", "askja_EnergyEl", "askja_TotalEnergy",
+    "askja_GaussLaw", "askja_UViol", "askja_WilsonLoop", "askja_PolyakovLoop", "askja_WilsonLoopDir",
+    "askja_PlaqExp", "askja_scalarLoopcorr", "askja_trajectory", "askja_run_trajectories", "askja_leapfrog",
+    "askja_md_steps", "askja_params_load", "askja_params_store", "askja_file_stem", "askja_conf_write",
+    "askja_conf_read", "askja_host_alloc", "askja_host_free",
+]
+
+
+class AskjaError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Params(ctypes.Structure):
+    _fields_ = [("nc", ctypes.c_int), ("dim", ctypes.c_int), ("n", ctypes.c_int * MAX_DIM),
+                ("beta", ctypes.c_double), ("dt", ctypes.c_double), ("level", ctypes.c_int),
+                ("precision", ctypes.c_int), ("reunitarise", ctypes.c_int), ("device", ctypes.c_int),
+                ("kernel_path", ctypes.c_int), ("seed", ctypes.c_uint64)]
+
+
+class TrajResult(ctypes.Structure):
+    _fields_ = [("h_old", ctypes.c_double), ("h_new", ctypes.c_double), ("dh", ctypes.c_double),
+                ("u", ctypes.c_double), ("accepted", ctypes.c_int), ("pad", ctypes.c_int),
+                ("traj", ctypes.c_ulonglong), ("n_acc", ctypes.c_ulonglong), ("n_acc1", ctypes.c_ulonglong),
+                ("n_rej", ctypes.c_ulonglong), ("n_tot", ctypes.c_ulonglong)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_ if f != "pad"}
+
+
+class RunParams(ctypes.Structure):
+    _fields_ = [("nc", ctypes.c_int), ("dim", ctypes.c_int), ("n", ctypes.c_int * MAX_DIM),
+                ("beta", ctypes.c_double), ("dt", ctypes.c_double)] + [
+        (k, ctypes.c_int) for k in ("steps", "update", "update2", "conftake", "level", "verbose", "runcontinue",
+                                    "random", "start", "taken", "nacc", "nac1", "nrec", "ntot")]
+
+    def as_dict(self):
+        d = {f: getattr(self, f) for f, _ in self._fields_ if f != "n"}
+        d["n"] = list(self.n)[: self.dim]
+        return d
+
+
+_lib = None
+
+
+def library() -> ctypes.CDLL:
+    """Load libaskja_b200.so (built in-tree by askja_b200.build)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise AskjaError(-5, f"{LIB_PATH} is not built; run `python -m askja_b200.build`")
+    L = ctypes.CDLL(LIB_PATH)
+    dp, vp, ip = ctypes.POINTER(ctypes.c_double), ctypes.c_void_p, ctypes.c_int
+    L.askja_create.argtypes = [ctypes.POINTER(Params), ctypes.POINTER(vp)]
+    L.askja_destroy.argtypes = [vp]
+    L.askja_destroy.restype = None
+    L.askja_last_error.argtypes = [vp]
+    L.askja_last_error.restype = ctypes.c_char_p
+    L.askja_version.restype = ctypes.c_char_p
+    L.askja_volume.argtypes = [vp]
+    L.askja_volume.restype = ctypes.c_long
+    L.askja_stream.argtypes = [vp]
+    L.askja_stream.restype = vp
+    for name in ("askja_sync", "askja_initializeU", "askja_copyDown", "askja_takeconfiguration",
+                 "askja_loadconfiguration", "askja_reunitarise"):
+        getattr(L, name).argtypes = [vp]
+    for name in ("askja_set_links", "askja_get_links", "askja_get_saved_links"):
+        getattr(L, name).argtypes = [vp, vp]
+    for name in ("askja_set_momenta", "askja_get_momenta"):
+        getattr(L, name).argtypes = [vp, ip, vp]
+    L.askja_hot_start.argtypes = [vp, ctypes.c_uint64]
+    L.askja_initializeE.argtypes = [vp, ctypes.c_uint64, ctypes.c_uint64]
+    for name in ("askja_updateE", "askja_updateUandcopyDown"):
+        getattr(L, name).argtypes = [vp, ctypes.c_double]
+    for name in ("askja_EnergyMag", "askja_EnergyEl", "askja_TotalEnergy", "askja_GaussLaw", "askja_UViol",
+                 "askja_WilsonLoop", "askja_PolyakovLoop", "askja_scalarLoopcorr"):
+        getattr(L, name).argtypes = [vp, dp]
+    L.askja_simpleenergyEl.argtypes = [vp, ip, dp]
+    L.askja_WilsonLoopDir.argtypes = [vp, ip, dp]
+    L.askja_PlaqExp.argtypes = [vp, dp, dp]
+    L.askja_trajectory.argtypes = [vp, ip, ctypes.POINTER(TrajResult)]
+    L.askja_run_trajectories.argtypes = [vp, ip, ip, ip, ctypes.POINTER(TrajResult), dp]
+    L.askja_leapfrog.argtypes = [vp, ip, ctypes.c_double]
+    L.askja_md_steps.argtypes = [vp, ip, ctypes.c_double]
+    L.askja_params_load.argtypes = [ctypes.c_char_p, ctypes.POINTER(RunParams)]
+    L.askja_params_store.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(RunParams), ip, ip]
+    L.askja_file_stem.argtypes = [ctypes.POINTER(RunParams), ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
+                                  ctypes.c_size_t]
+    L.askja_conf_write.argtypes = [ctypes.c_char_p, dp, ctypes.c_long]
+    L.askja_conf_read.argtypes = [ctypes.c_char_p, dp, ctypes.c_long]
+    L.askja_host_alloc.argtypes = [ctypes.c_size_t]
+    L.askja_host_alloc.restype = vp
+    L.askja_host_free.argtypes = [vp]
+    L.askja_host_free.restype = None
+    _lib = L
+    return L
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class Engine:
+    """One askja context: device copies of the reference's globals u, pi, Pi,
+    uconf for one lattice, plus a CUDA stream."""
+
+    def __init__(self, nc: int, dims, beta: float, dt: float = 0.02, level: int = 8, precision: str = "fp64",
+                 reunitarise: bool | None = None, device: int = 0, seed: int = 120351616, kernel_path: int = 0):
+        self.lib = library()
+        dims = [int(d) for d in dims]
+        p = Params()
+        p.nc, p.dim = int(nc), len(dims)
+        for i, d in enumerate(dims):
+            p.n[i] = d
+        p.beta, p.dt, p.level = float(beta), float(dt), int(level)
+        p.precision = {"fp64": FP64, "fp32": FP32}[precision]
+        p.reunitarise = -1 if reunitarise is None else int(bool(reunitarise))
+        p.device, p.kernel_path, p.seed = int(device), int(kernel_path), int(seed)
+        self.params = p
+        self._ctx = ctypes.c_void_p()
+        rc = self.lib.askja_create(ctypes.byref(p), ctypes.byref(self._ctx))
+        if rc != ASKJA_OK:
+            raise AskjaError(rc, self.lib.askja_last_error(None).decode())
+        self.nc, self.dims, self.dim = int(nc), dims, len(dims)
+        self.vol = int(np.prod(dims))
+        self.beta, self.dt, self.level, self.precision = float(beta), float(dt), int(level), precision
+
+    # -- plumbing --------------------------------------------------------
+    @property
+    def shape(self):
+        return (self.vol, self.dim, self.nc, self.nc)
+
+    def _ck(self, rc: int):
+        if rc != ASKJA_OK:
+            raise AskjaError(rc, self.lib.askja_last_error(self._ctx).decode())
+
+    def close(self):
+        if self._ctx:
+            self.lib.askja_destroy(self._ctx)
+            self._ctx = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def stream_ptr(self) -> int:
+        return int(self.lib.askja_stream(self._ctx) or 0)
+
+    def sync(self):
+        self._ck(self.lib.askja_sync(self._ctx))
+
+    def _host(self, x):
+        x = np.ascontiguousarray(x, dtype=np.complex128).reshape(self.shape)
+        return x
+
+    # -- fields ------------------------------------------------------------
+    def set_links(self, u):
+        u = self._host(u)
+        self._ck(self.lib.askja_set_links(self._ctx, u.ctypes.data))
+
+    def set_links_ptr(self, ptr: int):
+        """Upload links from a raw host pointer (e.g. pinned memory)."""
+        self._ck(self.lib.askja_set_links(self._ctx, ctypes.c_void_p(ptr)))
+
+    def get_links(self):
+        out = np.empty(self.shape, np.complex128)
+        self._ck(self.lib.askja_get_links(self._ctx, out.ctypes.data))
+        return out
+
+    def get_saved_links(self):
+        out = np.empty(self.shape, np.complex128)
+        self._ck(self.lib.askja_get_saved_links(self._ctx, out.ctypes.data))
+        return out
+
+    def set_momenta(self, p, which: int = 0):
+        p = self._host(p)
+        self._ck(self.lib.askja_set_momenta(self._ctx, int(which), p.ctypes.data))
+
+    def get_momenta(self, which: int = 0):
+        out = np.empty(self.shape, np.complex128)
+        self._ck(self.lib.askja_get_momenta(self._ctx, int(which), out.ctypes.data))
+        return out
+
+    def initializeU(self):
+        self._ck(self.lib.askja_initializeU(self._ctx))
+
+    def hot_start(self, seed: int):
+        self._ck(self.lib.askja_hot_start(self._ctx, int(seed)))
+
+    def initializeE(self, seed: int, counter: int = 0):
+        self._ck(self.lib.askja_initializeE(self._ctx, int(seed), int(counter)))
+
+    # -- the reference seam -------------------------------------------------
+    def updateE(self, eps: float):
+        self._ck(self.lib.askja_updateE(self._ctx, float(eps)))
+
+    def updateUandcopyDown(self, eps: float):
+        self._ck(self.lib.askja_updateUandcopyDown(self._ctx, float(eps)))
+
+    def copyDown(self):
+        self._ck(self.lib.askja_copyDown(self._ctx))
+
+    def takeconfiguration(self):
+        self._ck(self.lib.askja_takeconfiguration(self._ctx))
+
+    def loadconfiguration(self):
+        self._ck(self.lib.askja_loadconfiguration(self._ctx))
+
+    def reunitarise(self):
+        self._ck(self.lib.askja_reunitarise(self._ctx))
+
+    def _scalar(self, fn, *args):
+        v = ctypes.c_double()
+        self._ck(fn(self._ctx, *args, ctypes.byref(v)))
+        return v.value
+
+    def EnergyMag(self):
+        return self._scalar(self.lib.askja_EnergyMag)
+
+    def simpleenergyEl(self, which: int = 0):
+        return self._scalar(self.lib.askja_simpleenergyEl, int(which))
+
+    def EnergyEl(self):
+        return self._scalar(self.lib.askja_EnergyEl)
+
+    def TotalEnergy(self):
+        return self._scalar(self.lib.askja_TotalEnergy)
+
+    def GaussLaw(self):
+        return self._scalar(self.lib.askja_GaussLaw)
+
+    def UViol(self):
+        return self._scalar(self.lib.askja_UViol)
+
+    def WilsonLoop(self):
+        """sun.cpp's WilsonLoop: the line along dir 0 from site 0."""
+        return self._scalar(self.lib.askja_WilsonLoop)
+
+    def PolyakovLoop(self):
+        return self._scalar(self.lib.askja_PolyakovLoop)
+
+    def WilsonLoopDir(self, d: int):
+        return self._scalar(self.lib.askja_WilsonLoopDir, int(d))
+
+    def PlaqExp(self):
+        t, s = ctypes.c_double(), ctypes.c_double()
+        self._ck(self.lib.askja_PlaqExp(self._ctx, ctypes.byref(t), ctypes.byref(s)))
+        return t.value, s.value
+
+    def scalarLoopcorr(self):
+        out = np.zeros(self.dims[0])
+        self._ck(self.lib.askja_scalarLoopcorr(self._ctx, _dptr(out)))
+        return out
+
+    def hamiltonian(self, which: int = 0):
+        """beta * (EnergyMag + simpleenergyEl / (2 NC)), sun.cpp:1175/1254."""
+        return self.beta * (self.EnergyMag() + self.simpleenergyEl(which) / (2 * self.nc))
+
+    # -- trajectories ---------------------------------------------------------
+    def trajectory(self, nsteps: int) -> dict:
+        r = TrajResult()
+        self._ck(self.lib.askja_trajectory(self._ctx, int(nsteps), ctypes.byref(r)))
+        return r.as_dict()
+
+    def run_trajectories(self, ntraj: int, nsteps: int, use_graph: bool = True, want_log: bool = True):
+        r = TrajResult()
+        log = np.zeros(4 * max(ntraj, 1)) if want_log else None
+        self._ck(self.lib.askja_run_trajectories(self._ctx, int(ntraj), int(nsteps), int(bool(use_graph)),
+                                                 ctypes.byref(r), _dptr(log) if log is not None else None))
+        return r.as_dict(), (log.reshape(-1, 4)[:ntraj] if log is not None else None)
+
+    def leapfrog(self, nsteps: int, eps: float):
+        self._ck(self.lib.askja_leapfrog(self._ctx, int(nsteps), float(eps)))
+
+    def md_steps(self, nsteps: int, eps: float):
+        self._ck(self.lib.askja_md_steps(self._ctx, int(nsteps), float(eps)))
+
+
+# -- host I/O (no GPU needed) ---------------------------------------------------
+def params_load(path: str) -> dict:
+    L = library()
+    rp = RunParams()
+    rc = L.askja_params_load(path.encode(), ctypes.byref(rp))
+    if rc != ASKJA_OK:
+        raise AskjaError(rc, f"cannot load params file {path}")
+    return rp.as_dict()
+
+
+def _run_params(d: dict) -> RunParams:
+    rp = RunParams()
+    for k, _ in RunParams._fields_:
+        if k == "n":
+            for i, v in enumerate(d["n"]):
+                rp.n[i] = int(v)
+        elif k in d:
+            setattr(rp, k, d[k])
+    return rp
+
+
+def params_store(infile: str, outfile: str, d: dict, timestep: int, taken: int):
+    L = library()
+    rp = _run_params(d)
+    rc = L.askja_params_store(infile.encode(), outfile.encode(), ctypes.byref(rp), int(timestep), int(taken))
+    if rc != ASKJA_OK:
+        raise AskjaError(rc, f"cannot store params {infile} -> {outfile}")
+
+
+def file_stem(d: dict, directory: str, kind: str) -> str:
+    L = library()
+    rp = _run_params(d)
+    buf = ctypes.create_string_buffer(1024)
+    rc = L.askja_file_stem(ctypes.byref(rp), directory.encode(), kind.encode(), buf, 1024)
+    if rc != ASKJA_OK:
+        raise AskjaError(rc, "file stem")
+    return buf.value.decode()
+
+
+def conf_write(path: str, conf: np.ndarray):
+    L = library()
+    a = np.ascontiguousarray(conf, dtype=np.complex128).view(np.float64)
+    rc = L.askja_conf_write(path.encode(), _dptr(a), a.size)
+    if rc != ASKJA_OK:
+        raise AskjaError(rc, f"cannot write {path}")
+
+
+def conf_read(path: str, shape) -> np.ndarray:
+    L = library()
+    out = np.empty(shape, np.complex128)
+    a = out.view(np.float64)
+    rc = L.askja_conf_read(path.encode(), _dptr(a), a.size)
+    if rc != ASKJA_OK:
+        raise AskjaError(rc, f"cannot read {path}")
+    return out
+
+
+@dataclass
+class PinnedBuffer:
+    """Page-locked host buffer from askja_host_alloc (cudaMallocHost)."""
+    ptr: int
+    nbytes: int
+
+    @classmethod
+    def alloc(cls, nbytes: int) -> "PinnedBuffer":
+        p = library().askja_host_alloc(int(nbytes))
+        if not p:
+            raise AskjaError(-2, "askja_host_alloc failed")
+        return cls(int(p), int(nbytes))
+
+    def array(self, dtype, shape):
+        buf = (ctypes.c_char * self.nbytes).from_address(self.ptr)
+        return np.frombuffer(buf, dtype=dtype).reshape(shape)
+
+    def free(self):
+        if self.ptr:
+            library().askja_host_free(ctypes.c_void_p(self.ptr))
+            self.ptr = 0

@@ -1,0 +1,631 @@
+// askja B200 engine: context, device fields, and the C ABI of include/askja_gpu.h.
+//
+// Device state per context (all in HBM, SoA layout of common.cuh):
+//   U[0], U[1]  link field and its ping-pong partner (fused kick+drift writes
+//               the updated links to the other buffer, because neighbouring
+//               links are still being read)   -> the reference's u (and U)
+//   P           current momenta                -> pi
+//   P2          updated momenta                -> Pi
+//   Uconf       last accepted configuration    -> uconf
+//   nbr         periodic neighbour tables, 2*D planes of V int32
+//   partial/sums/st/log  reduction scratch and trajectory bookkeeping
+#include <cuda_runtime.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "../../include/askja_gpu.h"
+#include "launch.h"
+#include "misc.cuh"
+
+using askja::KernelSet;
+using askja::Lat;
+using askja::LaunchCtx;
+using askja::misc::TrajState;
+
+static_assert(sizeof(askja_traj_result) == sizeof(TrajState), "traj result layout");
+
+static thread_local std::string g_last_error;
+
+struct askja_ctx {
+  askja_params p{};
+  Lat lat{};
+  const KernelSet* ks = nullptr;
+  LaunchCtx lc{};
+  long V = 0, nl = 0;
+  int N = 0, D = 0;
+  size_t field_bytes = 0;
+  void* U[2] = {nullptr, nullptr};
+  int cur = 0;
+  void* P = nullptr;
+  void* P2 = nullptr;
+  void* Uconf = nullptr;
+  int* nbr = nullptr;
+  double* partial = nullptr;
+  double* sums = nullptr;   // [0..1] plaq t/s, [2..4] link sums, [5] gauss, [6..] line results
+  double* lines = nullptr;  // per-line results
+  TrajState* st = nullptr;
+  double* logbuf = nullptr;
+  int logcap = 0;
+  void* staging = nullptr;  // U-conf layout staging buffer (V*D*NC*NC double2)
+  unsigned long long* nonfinite = nullptr;
+  cudaStream_t stream = nullptr;
+  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  int g_nsteps[2] = {-1, -1};
+  std::string err;
+};
+
+namespace {
+
+int set_err(askja_ctx* c, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (c)
+    c->err = buf;
+  else
+    g_last_error = buf;
+  return code;
+}
+
+#define CK(call)                                                                                      \
+  do {                                                                                                \
+    cudaError_t e_ = (call);                                                                          \
+    if (e_ != cudaSuccess) return set_err(c, ASKJA_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+  } while (0)
+
+struct DevGuard {
+  explicit DevGuard(int dev) { cudaSetDevice(dev); }
+};
+
+// neighbour tables from the reference's coordinate scheme (structs.h:169-218)
+void build_neighbours(const askja_params& p, long V, std::vector<int>& nbr) {
+  long stride[ASKJA_MAX_DIM];
+  for (int i = 0; i < p.dim; i++) {
+    stride[i] = 1;
+    for (int j = i + 1; j < p.dim; j++) stride[i] *= p.n[j];
+  }
+  nbr.assign((size_t)2 * p.dim * V, 0);
+  for (int d = 0; d < p.dim; d++)
+    for (long s = 0; s < V; s++) {
+      const long c = (d == 0) ? s / stride[0] : (s % stride[d - 1]) / stride[d];
+      const long up = (c + 1) % p.n[d];
+      long dn = (c - 1) % p.n[d];
+      if (dn < 0) dn += p.n[d];
+      nbr[(size_t)(2 * d) * V + s] = (int)(s + (up - c) * stride[d]);
+      nbr[(size_t)(2 * d + 1) * V + s] = (int)(s + (dn - c) * stride[d]);
+    }
+}
+
+int scal(askja_ctx* c, const double* dev, double* host, int n) {
+  CK(cudaMemcpyAsync(host, dev, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return ASKJA_OK;
+}
+
+int check_ctx(askja_ctx* c) {
+  if (!c) return set_err(nullptr, ASKJA_ERR_ARG, "null context");
+  return ASKJA_OK;
+}
+
+void* cur_u(askja_ctx* c) { return c->U[c->cur]; }
+
+int launch_ok(askja_ctx* c, cudaError_t e, const char* what) {
+  if (e != cudaSuccess) return set_err(c, ASKJA_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+  return ASKJA_OK;
+}
+
+#define KL(expr, what)                            \
+  do {                                            \
+    int rc_ = launch_ok(c, (expr), what);         \
+    if (rc_) return rc_;                          \
+  } while (0)
+
+// Enqueue one whole trajectory (no host synchronisation; graph-capturable).
+int enqueue_trajectory(askja_ctx* c, int nsteps) {
+  const double dt = c->p.dt;
+  const double scale = std::sqrt(2.0 * c->N / c->p.beta);
+  KL(c->ks->refresh(c->lc, c->P, c->p.seed, &c->st->traj, 0, scale), "refresh");
+  KL(c->ks->plaq(c->lc, cur_u(c), c->partial, c->sums), "plaq");
+  KL(c->ks->linksums(c->lc, c->P, nullptr, nullptr, c->partial, c->sums + 2), "kinetic");
+  askja::misc::k_energy<<<1, 1, 0, c->stream>>>(c->sums, c->p.beta, c->N, &c->st->h_old);
+  KL(cudaGetLastError(), "energy");
+  for (int i = 0; i < nsteps; i++) {
+    KL(c->ks->force(c->lc, 1, cur_u(c), c->P, c->P, c->U[1 - c->cur], i == 0 ? 0.5 * dt : dt, dt), "kick+drift");
+    c->cur ^= 1;
+  }
+  KL(c->ks->force(c->lc, 0, cur_u(c), c->P, c->P, nullptr, 0.5 * dt, 0.0), "kick");
+  KL(c->ks->plaq(c->lc, cur_u(c), c->partial, c->sums), "plaq");
+  KL(c->ks->linksums(c->lc, c->P, nullptr, nullptr, c->partial, c->sums + 2), "kinetic");
+  askja::misc::k_energy<<<1, 1, 0, c->stream>>>(c->sums, c->p.beta, c->N, &c->st->h_new);
+  askja::misc::k_metropolis<<<1, 1, 0, c->stream>>>(c->st, c->p.seed, c->logbuf, c->logcap);
+  askja::misc::k_accept_copy<<<4 * 148, 256, 0, c->stream>>>(c->st, (uint4*)cur_u(c), (uint4*)c->Uconf,
+                                                             (long)(c->field_bytes / 16));
+  KL(cudaGetLastError(), "metropolis");
+  return ASKJA_OK;
+}
+
+void drop_graphs(askja_ctx* c) {
+  for (int i = 0; i < 2; i++) {
+    if (c->gexec[i]) cudaGraphExecDestroy(c->gexec[i]);
+    c->gexec[i] = nullptr;
+    c->g_nsteps[i] = -1;
+  }
+}
+
+int read_state(askja_ctx* c, askja_traj_result* out) {
+  if (!out) return ASKJA_OK;
+  CK(cudaMemcpyAsync(out, c->st, sizeof(TrajState), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return ASKJA_OK;
+}
+
+int upload_conf(askja_ctx* c, const double* conf, void* dst) {
+  const size_t bytes = (size_t)c->nl * c->N * c->N * 2 * sizeof(double);
+  CK(cudaMemcpyAsync(c->staging, conf, bytes, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemsetAsync(c->nonfinite, 0, sizeof(unsigned long long), c->stream));
+  askja::misc::k_count_nonfinite<<<4 * 148, 256, 0, c->stream>>>((const double*)c->staging,
+                                                                  (long)(bytes / sizeof(double)), c->nonfinite);
+  unsigned long long bad = 0;
+  CK(cudaMemcpyAsync(&bad, c->nonfinite, sizeof bad, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (bad) return set_err(c, ASKJA_ERR_NONFINITE, "input buffer holds %llu non-finite values", bad);
+  KL(c->ks->from_conf(c->lc, c->staging, dst), "from_conf");
+  return ASKJA_OK;
+}
+
+int download_conf(askja_ctx* c, const void* src, double* conf) {
+  const size_t bytes = (size_t)c->nl * c->N * c->N * 2 * sizeof(double);
+  KL(c->ks->to_conf(c->lc, src, c->staging), "to_conf");
+  CK(cudaMemcpyAsync(conf, c->staging, bytes, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return ASKJA_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* askja_version(void) { return "askja-b200 0.1 (sm_100a)"; }
+
+const char* askja_last_error(const askja_ctx* c) { return c ? c->err.c_str() : g_last_error.c_str(); }
+
+long askja_volume(const askja_ctx* c) { return c ? c->V : -1; }
+
+void* askja_stream(askja_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+int askja_sync(askja_ctx* c) {
+  if (int rc = check_ctx(c)) return rc;
+  DevGuard g(c->p.device);
+  CK(cudaStreamSynchronize(c->stream));
+  return ASKJA_OK;
+}
+
+void askja_destroy(askja_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->p.device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  drop_graphs(c);
+  void* bufs[] = {c->U[0], c->U[1], c->P, c->P2, c->Uconf, c->nbr, c->partial, c->sums, c->lines,
+                  c->st,   c->logbuf, c->staging, c->nonfinite};
+  for (void* b : bufs)
+    if (b) cudaFree(b);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+int askja_create(const askja_params* p, askja_ctx** out) {
+  askja_ctx* c = nullptr;
+  if (!p || !out) return set_err(nullptr, ASKJA_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (p->nc < 2 || p->nc > ASKJA_MAX_NC) return set_err(nullptr, ASKJA_ERR_ARG, "NC=%d outside 2..%d", p->nc, ASKJA_MAX_NC);
+  if (p->dim < 1 || p->dim > ASKJA_MAX_DIM)
+    return set_err(nullptr, ASKJA_ERR_ARG, "DIM=%d outside 1..%d", p->dim, ASKJA_MAX_DIM);
+  long V = 1;
+  for (int i = 0; i < p->dim; i++) {
+    if (p->n[i] < 1) return set_err(nullptr, ASKJA_ERR_ARG, "N%d=%d must be >= 1", i, p->n[i]);
+    V *= p->n[i];
+    if (V > (1L << 30)) return set_err(nullptr, ASKJA_ERR_ARG, "volume too large");
+  }
+  if (!(p->beta > 0.0) || !std::isfinite(p->beta)) return set_err(nullptr, ASKJA_ERR_ARG, "BETA must be > 0");
+  if (p->precision != ASKJA_FP64 && p->precision != ASKJA_FP32)
+    return set_err(nullptr, ASKJA_ERR_ARG, "unknown precision %d", p->precision);
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return set_err(nullptr, ASKJA_ERR_NODEVICE, "no CUDA device available (the engine has no CPU fallback)");
+  if (p->device < 0 || p->device >= ndev) return set_err(nullptr, ASKJA_ERR_ARG, "device %d not present", p->device);
+
+  c = new askja_ctx();
+  c->p = *p;
+  DevGuard g(p->device);
+  c->N = p->nc;
+  c->D = p->dim;
+  c->V = V;
+  c->nl = V * p->dim;
+  c->ks = p->precision == ASKJA_FP64 ? &askja::kernels_fp64 : &askja::kernels_fp32;
+  const size_t elem = p->precision == ASKJA_FP64 ? 16 : 8;
+  c->field_bytes = (size_t)c->nl * c->N * c->N * elem;
+  Lat& L = c->lat;
+  L.V = (int)V;
+  L.D = p->dim;
+  L.N = p->nc;
+  for (int i = 0; i < p->dim; i++) {
+    L.n[i] = p->n[i];
+    long s = 1;
+    for (int j = i + 1; j < p->dim; j++) s *= p->n[j];
+    L.stride[i] = (int)s;
+  }
+  auto fail = [&](int rc) {
+    g_last_error = c->err;
+    askja_destroy(c);
+    return rc;
+  };
+#define CKC(call)                                                                                          \
+  do {                                                                                                     \
+    cudaError_t e_ = (call);                                                                               \
+    if (e_ != cudaSuccess) return fail(set_err(c, ASKJA_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_))); \
+  } while (0)
+  CKC(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  for (void** b : {&c->U[0], &c->U[1], &c->P, &c->P2, &c->Uconf}) CKC(cudaMalloc(b, c->field_bytes));
+  std::vector<int> nbr;
+  build_neighbours(*p, V, nbr);
+  CKC(cudaMalloc(&c->nbr, nbr.size() * sizeof(int)));
+  CKC(cudaMemcpy(c->nbr, nbr.data(), nbr.size() * sizeof(int), cudaMemcpyHostToDevice));
+  L.nbr = c->nbr;
+  CKC(cudaMalloc(&c->partial, askja::partial_doubles(L) * sizeof(double)));
+  CKC(cudaMalloc(&c->sums, 64 * sizeof(double)));
+  long maxlines = 1;
+  for (int i = 0; i < p->dim; i++) maxlines = std::max(maxlines, (long)p->n[i]);
+  CKC(cudaMalloc(&c->lines, (maxlines + 8) * sizeof(double)));
+  CKC(cudaMalloc(&c->st, sizeof(TrajState)));
+  CKC(cudaMemset(c->st, 0, sizeof(TrajState)));
+  c->logcap = 4096;
+  CKC(cudaMalloc(&c->logbuf, (size_t)4 * c->logcap * sizeof(double)));
+  CKC(cudaMalloc(&c->staging, (size_t)c->nl * c->N * c->N * 2 * sizeof(double)));
+  CKC(cudaMalloc(&c->nonfinite, sizeof(unsigned long long)));
+  for (void* b : {c->U[0], c->U[1], c->P, c->P2, c->Uconf}) CKC(cudaMemset(b, 0, c->field_bytes));
+  c->lc.lat = L;
+  c->lc.stream = c->stream;
+  c->lc.order = askja::taylor_order(p->level);
+  c->lc.reunit = p->reunitarise < 0 ? (p->precision == ASKJA_FP32) : (p->reunitarise != 0);
+  c->lc.force_rows = p->kernel_path == 1;
+  // cold start by default
+  if (c->ks->identity(c->lc, c->U[0]) != cudaSuccess) return fail(set_err(c, ASKJA_ERR_CUDA, "identity launch"));
+  CKC(cudaMemcpyAsync(c->Uconf, c->U[0], c->field_bytes, cudaMemcpyDeviceToDevice, c->stream));
+  CKC(cudaStreamSynchronize(c->stream));
+#undef CKC
+  *out = c;
+  return ASKJA_OK;
+}
+
+int askja_set_links(askja_ctx* c, const double* conf) {
+  if (int rc = check_ctx(c)) return rc;
+  if (!conf) return set_err(c, ASKJA_ERR_ARG, "null buffer");
+  DevGuard g(c->p.device);
+  if (int rc = upload_conf(c, conf, cur_u(c))) return rc;
+  CK(cudaMemcpyAsync(c->Uconf, cur_u(c), c->field_bytes, cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return ASKJA_OK;
+}
+
+int askja_get_links(askja_ctx* c, double* conf) {
+  if (int rc = check_ctx(c)) return rc;
+  if (!conf) return set_err(c, ASKJA_ERR_ARG, "null buffer");
+  DevGuard g(c->p.device);
+  return download_conf(c, cur_u(c), conf);
+}
+
+int askja_get_saved_links(askja_ctx* c, double* conf) {
+  if (int rc = check_ctx(c)) return rc;
+  if (!conf) return set_err(c, ASKJA_ERR_ARG, "null buffer");
+  DevGuard g(c->p.device);
+  return download_conf(c, c->Uconf, conf);
+}
+
+int askja_set_momenta(askja_ctx* c, int which, const double* conf) {
+  if (int rc = check_ctx(c)) return rc;
+  if (!conf || (which != 0 && which != 1)) return set_err(c, ASKJA_ERR_ARG, "bad momentum buffer selector");
+  DevGuard g(c->p.device);
+  if (int rc = upload_conf(c, conf, which ? c->P2 : c->P)) return rc;
+  CK(cudaStreamSynchronize(c->stream));
+  return ASKJA_OK;
+}
+
+int askja_get_momenta(askja_ctx* c, int which, double* conf) {
+  if (int rc = check_ctx(c)) return rc;
+  if (!conf || (which != 0 && which != 1)) return set_err(c, ASKJA_ERR_ARG, "bad momentum buffer selector");
+  DevGuard g(c->p.device);
+  return download_conf(c, which ? c->P2 : c->P, conf);
+}
+
+int askja_initializeU(askja_ctx* c) {
+  if (int rc = check_ctx(c)) return rc;
+  DevGuard g(c->p.device);
+  KL(c->ks->identity(c->lc, cur_u(c)), "identity");
+  CK(cudaMemcpyAsync(c->Uconf, cur_u(c), c->field_bytes, cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return ASKJA_OK;
+}
+
+int askja_hot_start(askja_ctx* c, uint64_t seed) {
+  if (int rc = check_ctx(c)) return rc;
+  DevGuard g(c->p.device);
+  KL(c->ks->gauss_matrices(c->lc, cur_u(c), seed), "gaussian matrices");
+  // Gram-Schmidt + determinant phase always, whatever the reunitarise setting
+  LaunchCtx lc = c->lc;
+  KL(c->ks->reunit(lc, cur_u(c)), "reunitarise");
+  CK(cudaMemcpyAsync(c->Uconf, cur_u(c), c->field_bytes, cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return ASKJA_OK;
+}
+
+int askja_initializeE(askja_ctx* c, uint64_t seed, uint64_t counter) {
+  if (int rc = check_ctx(c)) return rc;
+  DevGuard g(c->p.device);
+  const double scale = std::sqrt(2.0 * c->N / c->p.beta);
+  KL(c->ks->refresh(c->lc, c->P, seed, nullptr, (unsigned long long)counter, scale), "refresh");
+  CK(cudaStreamSynchronize(c->stream));
+  return ASKJA_OK;
+}
+
+int askja_updateE(askja_ctx* c, double eps) {
+  if (int rc = check_ctx(c)) return rc;
+  DevGuard g(c->p.device);
+  KL(c->ks->force(c->lc, 0, cur_u(c), c->P, c->P2, nullptr, eps, 0.0), "updateE");
+  CK(cudaStreamSynchronize(c->stream));
+  return ASKJA_OK;
+}
+
+int askja_updateUandcopyDown(askja_ctx* c, double eps) {
+  if (int rc = check_ctx(c)) return rc;
+  DevGuard g(c->p.device);
+  KL(c->ks->drift(c->lc, cur_u(c), c->P2, eps), "drift");
+  CK(cudaMemcpyAsync(c->P, c->P2, c->field_bytes, cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return ASKJA_OK;
+}
+
+int askja_copyDown(askja_ctx* c) {
+  if (int rc = check_ctx(c)) return rc;
+  DevGuard g(c->p.device);
+  CK(cudaMemcpyAsync(c->P, c->P2, c->field_bytes, cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return ASKJA_OK;
+}
+
+int askja_takeconfiguration(askja_ctx* c) {
+  if (int rc = check_ctx(c)) return rc;
+  DevGuard g(c->p.device);
+  CK(cudaMemcpyAsync(c->Uconf, cur_u(c), c->field_bytes, cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return ASKJA_OK;
+}
+
+int askja_loadconfiguration(askja_ctx* c) {
+  if (int rc = check_ctx(c)) return rc;
+  DevGuard g(c->p.device);
+  CK(cudaMemcpyAsync(cur_u(c), c->Uconf, c->field_bytes, cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return ASKJA_OK;
+}
+
+int askja_reunitarise(askja_ctx* c) {
+  if (int rc = check_ctx(c)) return rc;
+  DevGuard g(c->p.device);
+  KL(c->ks->reunit(c->lc, cur_u(c)), "reunitarise");
+  CK(cudaStreamSynchronize(c->stream));
+  return ASKJA_OK;
+}
+
+int askja_PlaqExp(askja_ctx* c, double* temporal, double* spatial) {
+  if (int rc = check_ctx(c)) return rc;
+  DevGuard g(c->p.device);
+  KL(c->ks->plaq(c->lc, cur_u(c), c->partial, c->sums), "plaq");
+  double h[2];
+  if (int rc = scal(c, c->sums, h, 2)) return rc;
+  if (temporal) *temporal = h[0];
+  if (spatial) *spatial = h[1];
+  return ASKJA_OK;
+}
+
+int askja_EnergyMag(askja_ctx* c, double* out) {
+  double t = 0, s = 0;
+  if (int rc = askja_PlaqExp(c, &t, &s)) return rc;
+  if (!out) return set_err(c, ASKJA_ERR_ARG, "null output");
+  *out = t + s;
+  return ASKJA_OK;
+}
+
+static int linksums(askja_ctx* c, const void* Pa, const void* Pb, const void* U, double h[3]) {
+  DevGuard g(c->p.device);
+  KL(c->ks->linksums(c->lc, Pa, Pb, U, c->partial, c->sums + 2), "linksums");
+  return scal(c, c->sums + 2, h, 3);
+}
+
+int askja_simpleenergyEl(askja_ctx* c, int which, double* out) {
+  if (int rc = check_ctx(c)) return rc;
+  if (!out || (which != 0 && which != 1)) return set_err(c, ASKJA_ERR_ARG, "bad argument");
+  double h[3];
+  if (int rc = linksums(c, which ? c->P2 : c->P, nullptr, nullptr, h)) return rc;
+  *out = h[0];
+  return ASKJA_OK;
+}
+
+int askja_EnergyEl(askja_ctx* c, double* out) {
+  if (int rc = check_ctx(c)) return rc;
+  if (!out) return set_err(c, ASKJA_ERR_ARG, "null output");
+  double h[3];
+  if (int rc = linksums(c, c->P, c->P2, nullptr, h)) return rc;
+  *out = h[1];
+  return ASKJA_OK;
+}
+
+int askja_UViol(askja_ctx* c, double* out) {
+  if (int rc = check_ctx(c)) return rc;
+  if (!out) return set_err(c, ASKJA_ERR_ARG, "null output");
+  double h[3];
+  if (int rc = linksums(c, nullptr, nullptr, cur_u(c), h)) return rc;
+  *out = h[2];
+  return ASKJA_OK;
+}
+
+int askja_TotalEnergy(askja_ctx* c, double* out) {
+  double em = 0, el = 0;
+  if (int rc = askja_EnergyMag(c, &em)) return rc;
+  if (int rc = askja_EnergyEl(c, &el)) return rc;
+  if (!out) return set_err(c, ASKJA_ERR_ARG, "null output");
+  *out = 2.0 * c->N * em + el;
+  return ASKJA_OK;
+}
+
+int askja_GaussLaw(askja_ctx* c, double* out) {
+  if (int rc = check_ctx(c)) return rc;
+  if (!out) return set_err(c, ASKJA_ERR_ARG, "null output");
+  DevGuard g(c->p.device);
+  KL(c->ks->gauss(c->lc, cur_u(c), c->P2, c->partial, c->sums + 5), "gauss");
+  return scal(c, c->sums + 5, out, 1);
+}
+
+static int line_mean(askja_ctx* c, int dir, int nlines, int start_stride, double* out) {
+  DevGuard g(c->p.device);
+  KL(c->ks->lines(c->lc, cur_u(c), dir, nlines, start_stride, c->lines), "lines");
+  std::vector<double> h(nlines);
+  if (int rc = scal(c, c->lines, h.data(), nlines)) return rc;
+  double s = 0;
+  for (double v : h) s += v;
+  *out = s / nlines;
+  return ASKJA_OK;
+}
+
+int askja_WilsonLoop(askja_ctx* c, double* out) {
+  if (int rc = check_ctx(c)) return rc;
+  if (!out) return set_err(c, ASKJA_ERR_ARG, "null output");
+  return line_mean(c, 0, 1, 0, out);
+}
+
+int askja_PolyakovLoop(askja_ctx* c, double* out) {
+  if (int rc = check_ctx(c)) return rc;
+  if (!out) return set_err(c, ASKJA_ERR_ARG, "null output");
+  if (c->D < 2) return set_err(c, ASKJA_ERR_ARG, "PolyakovLoop needs DIM >= 2");
+  return line_mean(c, 0, c->lat.n[1], c->lat.stride[1], out);
+}
+
+int askja_WilsonLoopDir(askja_ctx* c, int dir, double* out) {
+  if (int rc = check_ctx(c)) return rc;
+  if (!out || dir < 1 || dir >= c->D) return set_err(c, ASKJA_ERR_ARG, "WilsonLoopDir needs 1 <= dir < DIM");
+  return line_mean(c, dir, c->lat.n[0], c->lat.stride[0], out);
+}
+
+int askja_scalarLoopcorr(askja_ctx* c, double* out) {
+  if (int rc = check_ctx(c)) return rc;
+  if (!out) return set_err(c, ASKJA_ERR_ARG, "null output");
+  DevGuard g(c->p.device);
+  KL(c->ks->slice_trace(c->lc, cur_u(c), c->lines), "slice trace");
+  return scal(c, c->lines, out, c->lat.n[0]);
+}
+
+int askja_leapfrog(askja_ctx* c, int nsteps, double eps) {
+  if (int rc = check_ctx(c)) return rc;
+  if (nsteps < 1) return set_err(c, ASKJA_ERR_ARG, "nsteps must be >= 1");
+  DevGuard g(c->p.device);
+  for (int i = 0; i < nsteps; i++) {
+    KL(c->ks->force(c->lc, 1, cur_u(c), c->P, c->P, c->U[1 - c->cur], i == 0 ? 0.5 * eps : eps, eps), "kick+drift");
+    c->cur ^= 1;
+  }
+  KL(c->ks->force(c->lc, 0, cur_u(c), c->P, c->P, nullptr, 0.5 * eps, 0.0), "kick");
+  CK(cudaStreamSynchronize(c->stream));
+  return ASKJA_OK;
+}
+
+int askja_md_steps(askja_ctx* c, int nsteps, double eps) {
+  if (int rc = check_ctx(c)) return rc;
+  if (nsteps < 0) return set_err(c, ASKJA_ERR_ARG, "nsteps must be >= 0");
+  if (nsteps == 0) return ASKJA_OK;
+  DevGuard g(c->p.device);
+  // D(eps) with Pi, pi = Pi ...
+  KL(c->ks->drift(c->lc, cur_u(c), c->P2, eps), "drift");
+  CK(cudaMemcpyAsync(c->P, c->P2, c->field_bytes, cudaMemcpyDeviceToDevice, c->stream));
+  // ... then (K D) fused, in place on pi ...
+  for (int i = 1; i < nsteps; i++) {
+    KL(c->ks->force(c->lc, 1, cur_u(c), c->P, c->P, c->U[1 - c->cur], eps, eps), "kick+drift");
+    c->cur ^= 1;
+  }
+  // ... and the last kick out of place: Pi = pi - eps F(u)
+  KL(c->ks->force(c->lc, 0, cur_u(c), c->P, c->P2, nullptr, eps, 0.0), "kick");
+  CK(cudaStreamSynchronize(c->stream));
+  return ASKJA_OK;
+}
+
+int askja_trajectory(askja_ctx* c, int nsteps, askja_traj_result* out) {
+  if (int rc = check_ctx(c)) return rc;
+  if (nsteps < 1) return set_err(c, ASKJA_ERR_ARG, "nsteps must be >= 1");
+  DevGuard g(c->p.device);
+  if (int rc = enqueue_trajectory(c, nsteps)) return rc;
+  CK(cudaStreamSynchronize(c->stream));
+  return read_state(c, out);
+}
+
+int askja_run_trajectories(askja_ctx* c, int ntraj, int nsteps, int use_graph, askja_traj_result* last,
+                           double* log) {
+  if (int rc = check_ctx(c)) return rc;
+  if (nsteps < 1 || ntraj < 0) return set_err(c, ASKJA_ERR_ARG, "bad trajectory counts");
+  DevGuard g(c->p.device);
+  TrajState st0;
+  CK(cudaMemcpyAsync(&st0, c->st, sizeof st0, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  for (int t = 0; t < ntraj; t++) {
+    if (!use_graph) {
+      if (int rc = enqueue_trajectory(c, nsteps)) return rc;
+      continue;
+    }
+    const int start = c->cur;
+    if (!c->gexec[start] || c->g_nsteps[start] != nsteps) {
+      if (c->gexec[start]) cudaGraphExecDestroy(c->gexec[start]);
+      c->gexec[start] = nullptr;
+      cudaGraph_t graph;
+      CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+      int rc = enqueue_trajectory(c, nsteps);
+      cudaError_t ce = cudaStreamEndCapture(c->stream, &graph);
+      c->cur = start;
+      if (rc) return rc;
+      if (ce != cudaSuccess) return set_err(c, ASKJA_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+      ce = cudaGraphInstantiate(&c->gexec[start], graph, 0);
+      cudaGraphDestroy(graph);
+      if (ce != cudaSuccess) return set_err(c, ASKJA_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ce));
+      c->g_nsteps[start] = nsteps;
+    }
+    CK(cudaGraphLaunch(c->gexec[start], c->stream));
+    c->cur = start ^ (nsteps & 1);
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  if (int rc = read_state(c, last)) return rc;
+  if (log && ntraj > 0) {
+    std::vector<double> ring((size_t)4 * c->logcap);
+    CK(cudaMemcpy(ring.data(), c->logbuf, ring.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    for (int t = 0; t < ntraj; t++) {
+      const unsigned long long k = (st0.traj + (unsigned long long)t) % (unsigned long long)c->logcap;
+      // only the last logcap trajectories are kept
+      if (ntraj - t > c->logcap) continue;
+      memcpy(log + 4 * (size_t)t, ring.data() + 4 * k, 4 * sizeof(double));
+    }
+  }
+  return ASKJA_OK;
+}
+
+void* askja_host_alloc(size_t bytes) {
+  void* p = nullptr;
+  if (cudaMallocHost(&p, bytes) != cudaSuccess) return nullptr;
+  return p;
+}
+
+void askja_host_free(void* p) {
+  if (p) cudaFreeHost(p);
+}
+
+}  // extern "C"

@@ -1,0 +1,278 @@
+// Template body of a KernelSet for one storage precision.  Included once by
+// kernels_fp64.cu (T = double) and once by kernels_fp32.cu (T = float).
+#pragma once
+
+#include <algorithm>
+
+#include "launch.h"
+#include "misc.cuh"
+#include "rows.cuh"
+#include "small.cuh"
+
+namespace askja {
+
+namespace detail {
+
+constexpr int SMALL_THREADS = 128;
+constexpr size_t ROWS_SMEM_BUDGET = 200 * 1024;
+
+inline long nlinks(const Lat& L) { return (long)L.V * L.D; }
+inline unsigned blocks_for(long n, int threads) { return (unsigned)((n + threads - 1) / threads); }
+
+template <typename T>
+struct Rows {
+  // groups per block and dynamic shared memory for the row-per-thread kernels
+  static void shape(int N, int* G, size_t* smem) {
+    const size_t per = rows::smem_per_group<T>(N);
+    int g = std::max(1, 128 / N);
+    g = std::min(g, 64);
+    while (g > 1 && (size_t)g * per > ROWS_SMEM_BUDGET) g--;
+    *G = g;
+    *smem = (size_t)g * per;
+  }
+};
+
+template <typename Kern>
+cudaError_t set_smem(Kern k, size_t smem) {
+  if (smem > 48 * 1024) return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  return cudaSuccess;
+}
+
+template <int NMAX, typename T>
+cudaError_t rows_force(const LaunchCtx& c, int mode, const void* U, const void* Pin, void* Pout, void* Uout,
+                       double ek, double ed) {
+  using S2 = typename Storage<T>::type;
+  int G;
+  size_t smem;
+  Rows<T>::shape(c.lat.N, &G, &smem);
+  const unsigned grid = blocks_for(nlinks(c.lat), G);
+  cudaError_t e;
+  if (mode == 0) {
+    auto k = rows::k_force<NMAX, T, S2, 0>;
+    if ((e = set_smem(k, smem)) != cudaSuccess) return e;
+    k<<<grid, G * c.lat.N, smem, c.stream>>>(c.lat, (const S2*)U, (const S2*)Pin, (S2*)Pout, (S2*)Uout, (T)ek, (T)ed,
+                                             c.order, c.reunit);
+  } else {
+    auto k = rows::k_force<NMAX, T, S2, 1>;
+    if ((e = set_smem(k, smem)) != cudaSuccess) return e;
+    k<<<grid, G * c.lat.N, smem, c.stream>>>(c.lat, (const S2*)U, (const S2*)Pin, (S2*)Pout, (S2*)Uout, (T)ek, (T)ed,
+                                             c.order, c.reunit);
+  }
+  return cudaGetLastError();
+}
+
+template <int NMAX, typename T>
+cudaError_t rows_drift(const LaunchCtx& c, void* U, const void* P, double eps) {
+  using S2 = typename Storage<T>::type;
+  int G;
+  size_t smem;
+  Rows<T>::shape(c.lat.N, &G, &smem);
+  auto k = rows::k_drift<NMAX, T, S2>;
+  cudaError_t e;
+  if ((e = set_smem(k, smem)) != cudaSuccess) return e;
+  k<<<blocks_for(nlinks(c.lat), G), G * c.lat.N, smem, c.stream>>>(c.lat, (S2*)U, (const S2*)P, (T)eps, c.order,
+                                                                     c.reunit);
+  return cudaGetLastError();
+}
+
+template <int N, typename T>
+cudaError_t small_force(const LaunchCtx& c, int mode, const void* U, const void* Pin, void* Pout, void* Uout,
+                        double ek, double ed) {
+  using S2 = typename Storage<T>::type;
+  const unsigned grid = blocks_for(nlinks(c.lat), SMALL_THREADS);
+  if (mode == 0)
+    small::k_force<N, T, S2, 0><<<grid, SMALL_THREADS, 0, c.stream>>>(c.lat, (const S2*)U, (const S2*)Pin, (S2*)Pout,
+                                                                      (S2*)Uout, (T)ek, (T)ed, c.order, c.reunit);
+  else
+    small::k_force<N, T, S2, 1><<<grid, SMALL_THREADS, 0, c.stream>>>(c.lat, (const S2*)U, (const S2*)Pin, (S2*)Pout,
+                                                                      (S2*)Uout, (T)ek, (T)ed, c.order, c.reunit);
+  return cudaGetLastError();
+}
+
+template <int N, typename T>
+cudaError_t small_drift(const LaunchCtx& c, void* U, const void* P, double eps) {
+  using S2 = typename Storage<T>::type;
+  small::k_drift<N, T, S2><<<blocks_for(nlinks(c.lat), SMALL_THREADS), SMALL_THREADS, 0, c.stream>>>(
+      c.lat, (S2*)U, (const S2*)P, (T)eps, c.order, c.reunit);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t force(const LaunchCtx& c, int mode, const void* U, const void* Pin, void* Pout, void* Uout, double ek,
+                  double ed) {
+  const int N = c.lat.N;
+  if (!c.force_rows) {
+    if (N == 2) return small_force<2, T>(c, mode, U, Pin, Pout, Uout, ek, ed);
+    if (N == 3) return small_force<3, T>(c, mode, U, Pin, Pout, Uout, ek, ed);
+    if (N == 4) return small_force<4, T>(c, mode, U, Pin, Pout, Uout, ek, ed);
+  }
+  if (N <= 8) return rows_force<8, T>(c, mode, U, Pin, Pout, Uout, ek, ed);
+  if (N <= 16) return rows_force<16, T>(c, mode, U, Pin, Pout, Uout, ek, ed);
+  if (N <= 32) return rows_force<32, T>(c, mode, U, Pin, Pout, Uout, ek, ed);
+  if (N <= 64) return rows_force<64, T>(c, mode, U, Pin, Pout, Uout, ek, ed);
+  return cudaErrorInvalidValue;
+}
+
+template <typename T>
+cudaError_t drift(const LaunchCtx& c, void* U, const void* P, double eps) {
+  const int N = c.lat.N;
+  if (!c.force_rows) {
+    if (N == 2) return small_drift<2, T>(c, U, P, eps);
+    if (N == 3) return small_drift<3, T>(c, U, P, eps);
+    if (N == 4) return small_drift<4, T>(c, U, P, eps);
+  }
+  if (N <= 8) return rows_drift<8, T>(c, U, P, eps);
+  if (N <= 16) return rows_drift<16, T>(c, U, P, eps);
+  if (N <= 32) return rows_drift<32, T>(c, U, P, eps);
+  if (N <= 64) return rows_drift<64, T>(c, U, P, eps);
+  return cudaErrorInvalidValue;
+}
+
+template <typename T>
+cudaError_t reunit(const LaunchCtx& c, void* U) {
+  using S2 = typename Storage<T>::type;
+  const int N = c.lat.N;
+  const unsigned gsm = blocks_for(nlinks(c.lat), SMALL_THREADS);
+  if (!c.force_rows) {
+    if (N == 2) {
+      small::k_reunit<2, T, S2><<<gsm, SMALL_THREADS, 0, c.stream>>>(c.lat, (S2*)U);
+      return cudaGetLastError();
+    }
+    if (N == 3) {
+      small::k_reunit<3, T, S2><<<gsm, SMALL_THREADS, 0, c.stream>>>(c.lat, (S2*)U);
+      return cudaGetLastError();
+    }
+    if (N == 4) {
+      small::k_reunit<4, T, S2><<<gsm, SMALL_THREADS, 0, c.stream>>>(c.lat, (S2*)U);
+      return cudaGetLastError();
+    }
+  }
+  int G;
+  size_t smem;
+  Rows<T>::shape(N, &G, &smem);
+  auto k = rows::k_reunit<T, S2>;
+  cudaError_t e;
+  if ((e = set_smem(k, smem)) != cudaSuccess) return e;
+  k<<<blocks_for(nlinks(c.lat), G), G * N, smem, c.stream>>>(c.lat, (S2*)U);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t plaq(const LaunchCtx& c, const void* U, double* partial, double* out) {
+  using S2 = typename Storage<T>::type;
+  const unsigned nb = blocks_for(c.lat.V, misc::RED_THREADS);
+  const int N = c.lat.N;
+  if (N == 2)
+    misc::k_plaq<2, S2><<<nb, misc::RED_THREADS, 0, c.stream>>>(c.lat, (const S2*)U, partial);
+  else if (N == 3)
+    misc::k_plaq<3, S2><<<nb, misc::RED_THREADS, 0, c.stream>>>(c.lat, (const S2*)U, partial);
+  else if (N == 4)
+    misc::k_plaq<4, S2><<<nb, misc::RED_THREADS, 0, c.stream>>>(c.lat, (const S2*)U, partial);
+  else
+    misc::k_plaq<0, S2><<<nb, misc::RED_THREADS, 0, c.stream>>>(c.lat, (const S2*)U, partial);
+  misc::k_finish<2><<<1, misc::RED_THREADS, 0, c.stream>>>(partial, (int)nb, out);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t linksums(const LaunchCtx& c, const void* Pa, const void* Pb, const void* U, double* partial, double* out) {
+  using S2 = typename Storage<T>::type;
+  const unsigned nb = blocks_for(nlinks(c.lat), misc::RED_THREADS);
+  const int N = c.lat.N;
+  if (N == 2)
+    misc::k_linksums<2, S2><<<nb, misc::RED_THREADS, 0, c.stream>>>(c.lat, (const S2*)Pa, (const S2*)Pb,
+                                                                    (const S2*)U, partial);
+  else if (N == 3)
+    misc::k_linksums<3, S2><<<nb, misc::RED_THREADS, 0, c.stream>>>(c.lat, (const S2*)Pa, (const S2*)Pb,
+                                                                    (const S2*)U, partial);
+  else if (N == 4)
+    misc::k_linksums<4, S2><<<nb, misc::RED_THREADS, 0, c.stream>>>(c.lat, (const S2*)Pa, (const S2*)Pb,
+                                                                    (const S2*)U, partial);
+  else
+    misc::k_linksums<0, S2><<<nb, misc::RED_THREADS, 0, c.stream>>>(c.lat, (const S2*)Pa, (const S2*)Pb,
+                                                                    (const S2*)U, partial);
+  misc::k_finish<3><<<1, misc::RED_THREADS, 0, c.stream>>>(partial, (int)nb, out);
+  return cudaGetLastError();
+}
+
+constexpr int GAUSS_LINKS_PER_BLOCK = 256;
+
+template <typename T>
+cudaError_t gauss(const LaunchCtx& c, const void* U, const void* Pi, double* partial, double* out) {
+  using S2 = typename Storage<T>::type;
+  const unsigned nb = blocks_for(nlinks(c.lat), GAUSS_LINKS_PER_BLOCK);
+  const int NN = c.lat.N * c.lat.N;
+  const int thr = std::min(misc::RED_THREADS, ((NN + 31) / 32) * 32);
+  misc::k_gauss<S2><<<nb, thr, 0, c.stream>>>(c.lat, (const S2*)U, (const S2*)Pi, GAUSS_LINKS_PER_BLOCK, partial);
+  misc::k_gauss_finish<<<1, thr, 2 * NN * sizeof(double), c.stream>>>(partial, (int)nb, c.lat.N, out);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t lines(const LaunchCtx& c, const void* U, int dir, int nlines, int start_stride, double* out) {
+  using S2 = typename Storage<T>::type;
+  const int N = c.lat.N;
+  const size_t smem = 2 * (size_t)N * N * sizeof(cpx<double>);
+  auto k = misc::k_lines<S2>;
+  cudaError_t e;
+  if ((e = set_smem(k, smem)) != cudaSuccess) return e;
+  k<<<nlines, ((N + 31) / 32) * 32, smem, c.stream>>>(c.lat, (const S2*)U, dir, start_stride, out);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t slice_trace(const LaunchCtx& c, const void* U, double* out) {
+  using S2 = typename Storage<T>::type;
+  misc::k_slice_trace<S2><<<c.lat.n[0], misc::RED_THREADS, 0, c.stream>>>(c.lat, (const S2*)U, out);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t refresh(const LaunchCtx& c, void* P, uint64_t seed, const unsigned long long* traj_dev,
+                    unsigned long long traj_host, double scale) {
+  using S2 = typename Storage<T>::type;
+  misc::k_refresh<S2><<<blocks_for(nlinks(c.lat), 128), 128, 0, c.stream>>>(c.lat, (S2*)P, seed, traj_dev, traj_host,
+                                                                              scale);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t identity(const LaunchCtx& c, void* U) {
+  using S2 = typename Storage<T>::type;
+  const long tot = nlinks(c.lat) * c.lat.N * c.lat.N;
+  misc::k_identity<S2><<<blocks_for(tot, 256), 256, 0, c.stream>>>(c.lat, (S2*)U);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t gauss_matrices(const LaunchCtx& c, void* U, uint64_t seed) {
+  using S2 = typename Storage<T>::type;
+  misc::k_gauss_matrices<S2><<<blocks_for(nlinks(c.lat), 128), 128, 0, c.stream>>>(c.lat, (S2*)U, seed);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t from_conf(const LaunchCtx& c, const void* conf, void* f) {
+  using S2 = typename Storage<T>::type;
+  const long tot = nlinks(c.lat) * c.lat.N * c.lat.N;
+  misc::k_from_conf<S2><<<blocks_for(tot, 256), 256, 0, c.stream>>>(c.lat, (const double2*)conf, (S2*)f);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t to_conf(const LaunchCtx& c, const void* f, void* conf) {
+  using S2 = typename Storage<T>::type;
+  const long tot = nlinks(c.lat) * c.lat.N * c.lat.N;
+  misc::k_to_conf<S2><<<blocks_for(tot, 256), 256, 0, c.stream>>>(c.lat, (const S2*)f, (double2*)conf);
+  return cudaGetLastError();
+}
+
+template <typename T>
+constexpr KernelSet make_set() {
+  return KernelSet{&force<T>,   &drift<T>,   &reunit<T>,  &plaq<T>,           &linksums<T>,  &gauss<T>, &lines<T>,
+                   &slice_trace<T>, &refresh<T>, &identity<T>, &gauss_matrices<T>, &from_conf<T>, &to_conf<T>};
+}
+
+}  // namespace detail
+
+}  // namespace askja

@@ -1,0 +1,18 @@
+// FP64 kernel table: the plain double-precision path (the reference's own
+// arithmetic, used for parity against the oracle).
+#include "kernels.cuh"
+
+namespace askja {
+
+const KernelSet kernels_fp64 = detail::make_set<double>();
+
+size_t partial_doubles(const Lat& L) {
+  const long nl = (long)L.V * L.D;
+  const size_t plaq = 2 * ((L.V + misc::RED_THREADS - 1) / misc::RED_THREADS);
+  const size_t links = 3 * ((nl + misc::RED_THREADS - 1) / misc::RED_THREADS);
+  const size_t gauss =
+      2 * (size_t)L.N * L.N * ((nl + detail::GAUSS_LINKS_PER_BLOCK - 1) / detail::GAUSS_LINKS_PER_BLOCK);
+  return std::max(plaq, std::max(links, gauss)) + 64;
+}
+
+}  // namespace askja

@@ -1,0 +1,51 @@
+// Host-side launch interface between the engine (engine.cu) and the kernels,
+// one table per storage precision (kernels_fp64.cu, kernels_fp32.cu).  Every
+// entry enqueues work on `stream` and returns the launch status.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "common.cuh"
+
+namespace askja {
+
+struct LaunchCtx {
+  Lat lat;
+  cudaStream_t stream;
+  int order;       // effective Taylor order
+  int reunit;      // reunitarise after each link update
+  int force_rows;  // use the row-per-thread kernels even for NC <= 4
+};
+
+// Scalar reductions return their values in device memory:
+//   plaq     -> out[0] temporal, out[1] spatial
+//   linksums -> out[0] sum tr2(Pa), out[1] sum 1/4 tr2(Pa+Pb), out[2] UViol
+//   gauss    -> out[0]
+struct KernelSet {
+  // mode 0: Pout = Pin - ek F(U); mode 1: also Uout = exp(i ed Pout) U
+  cudaError_t (*force)(const LaunchCtx&, int mode, const void* U, const void* Pin, void* Pout, void* Uout, double ek,
+                       double ed);
+  cudaError_t (*drift)(const LaunchCtx&, void* U, const void* P, double eps);
+  cudaError_t (*reunit)(const LaunchCtx&, void* U);
+  cudaError_t (*plaq)(const LaunchCtx&, const void* U, double* partial, double* out);
+  cudaError_t (*linksums)(const LaunchCtx&, const void* Pa, const void* Pb, const void* U, double* partial,
+                          double* out);
+  cudaError_t (*gauss)(const LaunchCtx&, const void* U, const void* Pi, double* partial, double* out);
+  cudaError_t (*lines)(const LaunchCtx&, const void* U, int dir, int nlines, int start_stride, double* out);
+  cudaError_t (*slice_trace)(const LaunchCtx&, const void* U, double* out);
+  cudaError_t (*refresh)(const LaunchCtx&, void* P, uint64_t seed, const unsigned long long* traj_dev,
+                         unsigned long long traj_host, double scale);
+  cudaError_t (*identity)(const LaunchCtx&, void* U);
+  cudaError_t (*gauss_matrices)(const LaunchCtx&, void* U, uint64_t seed);
+  cudaError_t (*from_conf)(const LaunchCtx&, const void* conf, void* f);
+  cudaError_t (*to_conf)(const LaunchCtx&, const void* f, void* conf);
+};
+
+// size (in doubles) of the partial buffer the reductions need
+size_t partial_doubles(const Lat& L);
+
+extern const KernelSet kernels_fp64;
+extern const KernelSet kernels_fp32;
+
+}  // namespace askja

@@ -1,0 +1,320 @@
+// Thread-per-link kernels for small colour number (NC <= 4): every matrix of
+// the staple sum lives in registers, one thread owns one link (d, s), and the
+// threads of a warp walk 32 consecutive sites of the same direction so every
+// element load is one coalesced 256 B (FP32) / 512 B (FP64) transaction.
+//
+// Physics follows the reference (sun.cpp, sunmat.h):
+//   force   F = Adjoint(U_mu(x) * sum_{nu != mu} [upper + lower staple])
+//           (sun.cpp:702-716, Adjoint = sunmat.h:355-371)
+//   kick    P <- P - eps * F
+//   drift   U <- exp(i eps P) U, Taylor order `order` in Horner form
+//           (sunmat.h:200-248, applied to U directly: U + X(U + X/2(U + ...)))
+// with the staple product factored as U_mu(x) * (sum of the remaining three
+// links), which saves one matrix product per staple against the reference's
+// left-to-right evaluation; results agree to rounding.
+#pragma once
+
+#include "common.cuh"
+
+namespace askja {
+namespace small {
+
+template <int N, typename T>
+struct Mat {
+  cpx<T> a[N][N];
+};
+
+template <int N, typename T, typename S2>
+__device__ __forceinline__ void load(Mat<N, T>& m, const S2* __restrict__ f, const Lat& L, int d, int s) {
+  const S2* p = f + (size_t)d * N * N * L.V + s;
+#pragma unroll
+  for (int i = 0; i < N; i++)
+#pragma unroll
+    for (int j = 0; j < N; j++) m.a[i][j] = ldc<T>(p + (size_t)(i * N + j) * L.V);
+}
+
+template <int N, typename T, typename S2>
+__device__ __forceinline__ void store(S2* __restrict__ f, const Mat<N, T>& m, const Lat& L, int d, int s) {
+  S2* p = f + (size_t)d * N * N * L.V + s;
+#pragma unroll
+  for (int i = 0; i < N; i++)
+#pragma unroll
+    for (int j = 0; j < N; j++) stc(p + (size_t)(i * N + j) * L.V, m.a[i][j]);
+}
+
+template <int N, typename T>
+__device__ __forceinline__ void zero(Mat<N, T>& m) {
+#pragma unroll
+  for (int i = 0; i < N; i++)
+#pragma unroll
+    for (int j = 0; j < N; j++) m.a[i][j] = czero<T>();
+}
+
+// C = A * B^dag
+template <int N, typename T>
+__device__ __forceinline__ void mul_nd(Mat<N, T>& C, const Mat<N, T>& A, const Mat<N, T>& B) {
+#pragma unroll
+  for (int i = 0; i < N; i++)
+#pragma unroll
+    for (int j = 0; j < N; j++) {
+      cpx<T> s = czero<T>();
+#pragma unroll
+      for (int k = 0; k < N; k++) cmac_nc(s, A.a[i][k], B.a[j][k]);
+      C.a[i][j] = s;
+    }
+}
+// C += A * B^dag
+template <int N, typename T>
+__device__ __forceinline__ void mac_nd(Mat<N, T>& C, const Mat<N, T>& A, const Mat<N, T>& B) {
+#pragma unroll
+  for (int i = 0; i < N; i++)
+#pragma unroll
+    for (int j = 0; j < N; j++)
+#pragma unroll
+      for (int k = 0; k < N; k++) cmac_nc(C.a[i][j], A.a[i][k], B.a[j][k]);
+}
+// C = A^dag * B^dag  (= (B A)^dag)
+template <int N, typename T>
+__device__ __forceinline__ void mul_dd(Mat<N, T>& C, const Mat<N, T>& A, const Mat<N, T>& B) {
+#pragma unroll
+  for (int i = 0; i < N; i++)
+#pragma unroll
+    for (int j = 0; j < N; j++) {
+      cpx<T> s = czero<T>();
+#pragma unroll
+      for (int k = 0; k < N; k++) cmac_cc(s, A.a[k][i], B.a[j][k]);
+      C.a[i][j] = s;
+    }
+}
+// C += A * B
+template <int N, typename T>
+__device__ __forceinline__ void mac_nn(Mat<N, T>& C, const Mat<N, T>& A, const Mat<N, T>& B) {
+#pragma unroll
+  for (int i = 0; i < N; i++)
+#pragma unroll
+    for (int j = 0; j < N; j++)
+#pragma unroll
+      for (int k = 0; k < N; k++) cmac(C.a[i][j], A.a[i][k], B.a[k][j]);
+}
+// C = A * B
+template <int N, typename T>
+__device__ __forceinline__ void mul_nn(Mat<N, T>& C, const Mat<N, T>& A, const Mat<N, T>& B) {
+#pragma unroll
+  for (int i = 0; i < N; i++)
+#pragma unroll
+    for (int j = 0; j < N; j++) {
+      cpx<T> s = czero<T>();
+#pragma unroll
+      for (int k = 0; k < N; k++) cmac(s, A.a[i][k], B.a[k][j]);
+      C.a[i][j] = s;
+    }
+}
+
+// Sum of the 2(D-1) staples around link (mu, x), without the leading U_mu(x):
+//   sum_{nu != mu} U_nu(x+mu) U_mu^dag(x+nu) U_nu^dag(x)
+//               + U_nu^dag(x+mu-nu) U_mu^dag(x-nu) U_nu(x-nu)
+template <int N, typename T, typename S2>
+__device__ __forceinline__ void staple_sum(Mat<N, T>& acc, const S2* __restrict__ U, const Lat& L, int mu, int x) {
+  zero(acc);
+  const int xpmu = nb_plus(L, mu, x);
+  for (int nu = 0; nu < L.D; nu++) {
+    if (nu == mu) continue;
+    const int xpnu = nb_plus(L, nu, x);
+    const int xmnu = nb_minus(L, nu, x);
+    const int xpmu_mnu = nb_minus(L, nu, xpmu);
+    {
+      Mat<N, T> A, B, T1;
+      load(A, U, L, nu, xpmu);
+      load(B, U, L, mu, xpnu);
+      mul_nd(T1, A, B);
+      load(A, U, L, nu, x);
+      mac_nd(acc, T1, A);
+    }
+    {
+      Mat<N, T> A, B, T1;
+      load(A, U, L, nu, xpmu_mnu);
+      load(B, U, L, mu, xmnu);
+      mul_dd(T1, A, B);
+      load(A, U, L, nu, xmnu);
+      mac_nn(acc, T1, A);
+    }
+  }
+}
+
+// P <- P - eps * Adjoint(W), Adjoint(W) = -i/2 [(W - W^dag) - Tr(W - W^dag)/N]
+template <int N, typename T>
+__device__ __forceinline__ void kick_ta(Mat<N, T>& P, const Mat<N, T>& W, T eps) {
+  T trim = T(0);
+#pragma unroll
+  for (int k = 0; k < N; k++) trim += W.a[k][k].im;
+  trim = trim / T(N);
+#pragma unroll
+  for (int i = 0; i < N; i++)
+#pragma unroll
+    for (int j = 0; j < N; j++) {
+      T fr, fi;
+      if (i == j) {
+        fr = W.a[i][i].im - trim;
+        fi = T(0);
+      } else {
+        fr = T(0.5) * (W.a[i][j].im + W.a[j][i].im);
+        fi = T(-0.5) * (W.a[i][j].re - W.a[j][i].re);
+      }
+      P.a[i][j].re = fma(-eps, fr, P.a[i][j].re);
+      P.a[i][j].im = fma(-eps, fi, P.a[i][j].im);
+    }
+}
+
+// Tm <- exp(i eps P) U to Taylor order `order` (Horner, applied to U)
+template <int N, typename T>
+__device__ __forceinline__ void expi_times(Mat<N, T>& Tm, const Mat<N, T>& P, const Mat<N, T>& Ux, T eps, int order) {
+  Mat<N, T> X;
+#pragma unroll
+  for (int i = 0; i < N; i++)
+#pragma unroll
+    for (int j = 0; j < N; j++) X.a[i][j] = mkc<T>(-eps * P.a[i][j].im, eps * P.a[i][j].re);
+  Tm = Ux;
+  for (int n = order; n >= 1; n--) {
+    const T inv = T(1) / T(n);
+    Mat<N, T> Y;
+#pragma unroll
+    for (int i = 0; i < N; i++)
+#pragma unroll
+      for (int j = 0; j < N; j++) {
+        cpx<T> s = czero<T>();
+#pragma unroll
+        for (int k = 0; k < N; k++) cmac(s, X.a[i][k], Tm.a[k][j]);
+        Y.a[i][j] = mkc<T>(fma(s.re, inv, Ux.a[i][j].re), fma(s.im, inv, Ux.a[i][j].im));
+      }
+    Tm = Y;
+  }
+}
+
+// Project onto SU(N): modified Gram-Schmidt of rows 0..N-2 (in order), then
+// the last row is the unique unit row that completes them to determinant 1
+// (the conjugated generalised cross product of the other rows).
+template <int N, typename T>
+__device__ __forceinline__ void reunitarise(Mat<N, T>& M) {
+#pragma unroll
+  for (int r = 0; r < N - 1; r++) {
+#pragma unroll
+    for (int q = 0; q < r; q++) {
+      cpx<T> pr = czero<T>();
+#pragma unroll
+      for (int k = 0; k < N; k++) cmac_cn(pr, M.a[q][k], M.a[r][k]);
+#pragma unroll
+      for (int k = 0; k < N; k++) {
+        M.a[r][k].re -= pr.re * M.a[q][k].re - pr.im * M.a[q][k].im;
+        M.a[r][k].im -= pr.re * M.a[q][k].im + pr.im * M.a[q][k].re;
+      }
+    }
+    T nrm = T(0);
+#pragma unroll
+    for (int k = 0; k < N; k++) nrm += M.a[r][k].re * M.a[r][k].re + M.a[r][k].im * M.a[r][k].im;
+    const T inv = T(1) / sqrt(nrm);
+#pragma unroll
+    for (int k = 0; k < N; k++) {
+      M.a[r][k].re *= inv;
+      M.a[r][k].im *= inv;
+    }
+  }
+  if (N == 1) {
+    M.a[0][0] = mkc<T>(T(1), T(0));
+  } else if (N == 2) {
+    // last row = (-conj(a01), conj(a00))
+    M.a[1][0] = mkc<T>(-M.a[0][1].re, M.a[0][1].im);
+    M.a[1][1] = mkc<T>(M.a[0][0].re, -M.a[0][0].im);
+  } else if (N == 3) {
+    // last row = conj(r0 x r1)
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      const int k1 = (k + 1) % 3, k2 = (k + 2) % 3;
+      cpx<T> c = czero<T>();
+      cmac(c, M.a[0][k1], M.a[1][k2]);
+      c.re -= M.a[0][k2].re * M.a[1][k1].re - M.a[0][k2].im * M.a[1][k1].im;
+      c.im -= M.a[0][k2].re * M.a[1][k1].im + M.a[0][k2].im * M.a[1][k1].re;
+      M.a[2][k] = mkc<T>(c.re, -c.im);
+    }
+  } else if (N == 4) {
+    // last row k = conj of cofactor C_{3k} of rows 0..2, so that det = sum_k a3k C3k = 1
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      int c0 = (k == 0) ? 1 : 0;
+      int c1 = (k <= 1) ? 2 : 1;
+      int c2 = (k <= 2) ? 3 : 2;
+      // 3x3 minor of rows 0..2, columns c0<c1<c2
+      cpx<T> m = czero<T>();
+      const int cols[3] = {c0, c1, c2};
+#pragma unroll
+      for (int p = 0; p < 3; p++) {
+        const int q1 = (p + 1) % 3, q2 = (p + 2) % 3;
+        cpx<T> t = czero<T>();
+        cmac(t, M.a[1][cols[q1]], M.a[2][cols[q2]]);
+        t.re -= M.a[1][cols[q2]].re * M.a[2][cols[q1]].re - M.a[1][cols[q2]].im * M.a[2][cols[q1]].im;
+        t.im -= M.a[1][cols[q2]].re * M.a[2][cols[q1]].im + M.a[1][cols[q2]].im * M.a[2][cols[q1]].re;
+        cmac(m, M.a[0][cols[p]], t);
+      }
+      const T sgn = ((3 + k) & 1) ? T(-1) : T(1);
+      M.a[3][k] = mkc<T>(sgn * m.re, -sgn * m.im);
+    }
+  }
+}
+
+// MODE 0: out-of-place kick        Pout = Pin - eps_k F(U)                (updateE)
+// MODE 1: fused kick + drift       P -= eps_k F(U); Uout = exp(i eps_d P) U
+template <int N, typename T, typename S2, int MODE>
+__global__ void __launch_bounds__(128) k_force(Lat L, const S2* __restrict__ U, const S2* Pin,
+                                               S2* Pout, S2* __restrict__ Uout, T eps_k, T eps_d,
+                                               int order, int reunit) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long)L.V * L.D) return;
+  const int mu = (int)(t / L.V);
+  const int x = (int)(t - (long)mu * L.V);
+  Mat<N, T> acc, Ux, W;
+  staple_sum<N, T, S2>(acc, U, L, mu, x);
+  load(Ux, U, L, mu, x);
+  mul_nn(W, Ux, acc);
+  Mat<N, T> P;
+  load(P, Pin, L, mu, x);
+  kick_ta(P, W, eps_k);
+  store(Pout, P, L, mu, x);
+  if (MODE == 1) {
+    Mat<N, T> Tm;
+    expi_times(Tm, P, Ux, eps_d, order);
+    if (reunit) reunitarise(Tm);
+    store(Uout, Tm, L, mu, x);
+  }
+}
+
+// In-place drift: U <- exp(i eps P) U (updateUandcopyDown; the copy pi = Pi is
+// done by the caller).  Optionally reunitarises.
+template <int N, typename T, typename S2>
+__global__ void __launch_bounds__(128) k_drift(Lat L, S2* __restrict__ U, const S2* __restrict__ P, T eps, int order,
+                                               int reunit) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long)L.V * L.D) return;
+  const int mu = (int)(t / L.V);
+  const int x = (int)(t - (long)mu * L.V);
+  Mat<N, T> Ux, Pm, Tm;
+  load(Ux, U, L, mu, x);
+  load(Pm, P, L, mu, x);
+  expi_times(Tm, Pm, Ux, eps, order);
+  if (reunit) reunitarise(Tm);
+  store(U, Tm, L, mu, x);
+}
+
+// In-place reunitarisation of every link.
+template <int N, typename T, typename S2>
+__global__ void __launch_bounds__(128) k_reunit(Lat L, S2* __restrict__ U) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long)L.V * L.D) return;
+  const int mu = (int)(t / L.V);
+  const int x = (int)(t - (long)mu * L.V);
+  Mat<N, T> Ux;
+  load(Ux, U, L, mu, x);
+  reunitarise(Ux);
+  store(U, Ux, L, mu, x);
+}
+
+}  // namespace small
+}  // namespace askja

@@ -1,0 +1,185 @@
+/*
+ * askja_gpu.h -- C ABI of the askja B200 engine (libaskja_b200.so).
+ *
+ * A drop-in for the HMC path of paro8929/askja.  The reference has no FFI: its
+ * in-process seam is a set of global-state functions in sun.cpp operating on
+ * the globals u, U, pi, Pi, uconf (sun.cpp:82-89).  Each entry point below
+ * names the reference routine it replaces.  A context owns the device copy of
+ * those globals plus one CUDA stream; all work is ordered on that stream.
+ *
+ * Conventions
+ *  - Every call returns ASKJA_OK (0) or a negative ASKJA_ERR_* status; the
+ *    message is available from askja_last_error().  Nothing aborts or exits
+ *    and no C++ exception crosses the ABI.  (The reference prints and sets a
+ *    global ABORT flag: sun.cpp:48, 934-935, 1053-1054.)
+ *  - Host field buffers use the reference's U-conf byte order
+ *    (sun.cpp:289-302, gsl_matrix_complex_fwrite per link):
+ *        [site][dir][row][col][re,im]   as doubles,
+ *    i.e. V*DIM*NC*NC*2 doubles, site index with x0 slowest
+ *    (structs.h:130-165).  Buffers are caller-owned and copied synchronously.
+ *  - There is no CPU fallback: askja_create fails when no CUDA device is
+ *    present or the kernels cannot load.
+ *  - One host thread per context.
+ */
+#ifndef ASKJA_GPU_H
+#define ASKJA_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define ASKJA_API __attribute__((visibility("default")))
+#else
+#define ASKJA_API
+#endif
+
+#define ASKJA_OK 0
+#define ASKJA_ERR_ARG (-1)         /* invalid argument or unsupported shape */
+#define ASKJA_ERR_CUDA (-2)        /* a CUDA call failed (message says which) */
+#define ASKJA_ERR_IO (-3)          /* file missing, short or unwritable */
+#define ASKJA_ERR_NONFINITE (-4)   /* NaN/Inf in an uploaded host buffer */
+#define ASKJA_ERR_NODEVICE (-5)    /* no CUDA device */
+#define ASKJA_ERR_PARSE (-6)       /* malformed params file */
+
+#define ASKJA_FP64 0 /* links, momenta and arithmetic in FP64 (the reference's precision) */
+#define ASKJA_FP32 1 /* FP32 links/momenta/arithmetic, reunitarised; FP64 reductions and dH */
+
+#define ASKJA_MAX_DIM 16
+#define ASKJA_MAX_NC 64
+
+typedef struct askja_ctx askja_ctx;
+
+/* Lattice and integrator settings: the params-file keys NC, DIM, N0..N{DIM-1},
+ * BETA, DT, LEVEL (sun.cpp:803-888) plus the engine's own precision/seed. */
+typedef struct {
+  int nc;              /* NC, 2..64 */
+  int dim;             /* DIM, 1..16 */
+  int n[ASKJA_MAX_DIM];/* N0..N{DIM-1}, each >= 1 */
+  double beta;         /* BETA */
+  double dt;           /* DT (used by askja_trajectory) */
+  int level;           /* LEVEL: Taylor order of exp(i dt P); outside 0..8 acts as 8 (sunmat.h:215-246) */
+  int precision;       /* ASKJA_FP64 or ASKJA_FP32 */
+  int reunitarise;     /* -1 default (on for FP32, off for FP64), 0 off, 1 on */
+  int device;          /* CUDA device ordinal */
+  int kernel_path;     /* 0 automatic; 1 row-per-thread kernels for every NC (testing) */
+  uint64_t seed;       /* Philox key for momenta, Metropolis uniforms and hot start */
+} askja_params;
+
+/* Outcome of one trajectory (sun.cpp:1249-1318). */
+typedef struct {
+  double h_old;        /* CRITENERGY: beta*(EnergyMag + simpleenergyEl(pi)/(2 NC)) before */
+  double h_new;        /* myenergy after the closing half kick */
+  double dh;           /* h_new - h_old */
+  double u;            /* Metropolis uniform */
+  int accepted;        /* 0 reject, 1 "ACCEPT case 1" (dH<0), 2 "ACCEPT case 2" */
+  int pad;
+  unsigned long long traj;                  /* trajectories run by this context */
+  unsigned long long n_acc, n_acc1, n_rej;  /* NACC, NAC1, NREC (sun.cpp:42-45) */
+  unsigned long long n_tot;                 /* NTOT */
+} askja_traj_result;
+
+/* ---- lifetime ---------------------------------------------------------- */
+/* Allocates the device fields (u, pi, Pi, uconf and a second link buffer) and
+ * neighbour tables; replaces allocate_memory/xygrid.init/generators
+ * (sun.cpp:96-125, structs.h:109-147, sun.cpp:142-189). */
+ASKJA_API int askja_create(const askja_params* p, askja_ctx** out);
+ASKJA_API void askja_destroy(askja_ctx* ctx);
+ASKJA_API const char* askja_last_error(const askja_ctx* ctx); /* ctx may be NULL: last create() error */
+ASKJA_API const char* askja_version(void);
+ASKJA_API long askja_volume(const askja_ctx* ctx);            /* V = prod N_d (xygrid.SIZE) */
+ASKJA_API void* askja_stream(askja_ctx* ctx);                 /* the context's cudaStream_t */
+ASKJA_API int askja_sync(askja_ctx* ctx);
+
+/* ---- fields (U-conf layout) ------------------------------------------- */
+/* u := conf and uconf := conf (loadconf + takeconfiguration, sun.cpp:744-765,
+ * 1164-1170).  Rejects non-finite input with ASKJA_ERR_NONFINITE. */
+ASKJA_API int askja_set_links(askja_ctx* ctx, const double* conf);
+ASKJA_API int askja_get_links(askja_ctx* ctx, double* conf);          /* current u */
+ASKJA_API int askja_get_saved_links(askja_ctx* ctx, double* conf);    /* uconf (what storeconf writes, sun.cpp:289-302) */
+/* which = 0: pi (current momenta), 1: Pi (updated momenta) */
+ASKJA_API int askja_set_momenta(askja_ctx* ctx, int which, const double* conf);
+ASKJA_API int askja_get_momenta(askja_ctx* ctx, int which, double* conf);
+ASKJA_API int askja_initializeU(askja_ctx* ctx);                       /* cold start, sun.cpp:194-207; also uconf */
+ASKJA_API int askja_hot_start(askja_ctx* ctx, uint64_t seed);          /* Haar SU(NC) links (not in the reference); also uconf */
+/* pi := sqrt(2NC/beta) sum_a xi_a T_a with Philox normals keyed by (seed,
+ * counter): replaces initializeE (sun.cpp:209-252), whose GSL stream is
+ * time-seeded and not reproducible. */
+ASKJA_API int askja_initializeE(askja_ctx* ctx, uint64_t seed, uint64_t counter);
+
+/* ---- the reference's in-process seam ---------------------------------- */
+ASKJA_API int askja_updateE(askja_ctx* ctx, double eps);              /* Pi = pi - eps*Adjoint(staples): sun.cpp:672-723 */
+ASKJA_API int askja_updateUandcopyDown(askja_ctx* ctx, double eps);   /* u = mexpi(eps*Pi,L)*u; pi = Pi: sun.cpp:774-790 */
+ASKJA_API int askja_copyDown(askja_ctx* ctx);                         /* pi = Pi: sun.cpp:792-801 */
+ASKJA_API int askja_takeconfiguration(askja_ctx* ctx);                /* uconf = u: sun.cpp:725-732 */
+ASKJA_API int askja_loadconfiguration(askja_ctx* ctx);                /* u = uconf: sun.cpp:734-742 */
+ASKJA_API int askja_reunitarise(askja_ctx* ctx);                      /* project u onto SU(NC) (not in the reference) */
+ASKJA_API int askja_EnergyMag(askja_ctx* ctx, double* out);           /* sun.cpp:507-537 */
+ASKJA_API int askja_simpleenergyEl(askja_ctx* ctx, int which, double* out); /* sun.cpp:540-548, which 0 = pi, 1 = Pi */
+ASKJA_API int askja_EnergyEl(askja_ctx* ctx, double* out);            /* sun.cpp:560-567 */
+ASKJA_API int askja_TotalEnergy(askja_ctx* ctx, double* out);         /* sun.cpp:571-576 */
+ASKJA_API int askja_GaussLaw(askja_ctx* ctx, double* out);            /* sun.cpp:415-438 */
+ASKJA_API int askja_UViol(askja_ctx* ctx, double* out);               /* sun.cpp:441-471 */
+ASKJA_API int askja_WilsonLoop(askja_ctx* ctx, double* out);          /* sun.cpp:307-362 (evs[0]) */
+
+/* ---- measure4d observables on the current u --------------------------- */
+ASKJA_API int askja_PolyakovLoop(askja_ctx* ctx, double* out);                 /* measurements4d.cpp:410-466 */
+ASKJA_API int askja_WilsonLoopDir(askja_ctx* ctx, int dir, double* out);       /* measurements4d.cpp:311-355 */
+ASKJA_API int askja_PlaqExp(askja_ctx* ctx, double* temporal, double* spatial);/* measurements4d.cpp:885-927 */
+ASKJA_API int askja_scalarLoopcorr(askja_ctx* ctx, double* out /* N0 values */); /* measurements4d.cpp:357-408 */
+
+/* ---- whole trajectories, on the device -------------------------------- */
+/* One HMC trajectory as in sun.cpp:1249-1318 with `nsteps` link updates:
+ * momentum refresh, H_old, half kick, (drift, kick) x nsteps with the last
+ * kick halved, H_new, Metropolis, then uconf = u (accept) or u = uconf
+ * (reject).  No host synchronisation inside. */
+ASKJA_API int askja_trajectory(askja_ctx* ctx, int nsteps, askja_traj_result* out);
+/* `ntraj` trajectories; with use_graph != 0 each is a CUDA-graph replay.
+ * `log` (may be NULL) receives 4 doubles per trajectory: h_old, h_new, dh, accepted. */
+ASKJA_API int askja_run_trajectories(askja_ctx* ctx, int ntraj, int nsteps, int use_graph, askja_traj_result* last,
+                           double* log);
+/* Only the leapfrog part of askja_trajectory (refresh, H and Metropolis
+ * excluded): K(eps/2) [D(eps) K(eps)]^(nsteps-1) D(eps) K(eps/2) with fused
+ * kick+drift kernels. */
+ASKJA_API int askja_leapfrog(askja_ctx* ctx, int nsteps, double eps);
+
+/* `nsteps` repetitions of the reference's inner MD step
+ * "updateUandcopyDown(eps); updateE(eps)" (sun.cpp:1216-1218), computed with
+ * fused kick+drift kernels; afterwards pi and Pi hold exactly what the
+ * reference's globals would. */
+ASKJA_API int askja_md_steps(askja_ctx* ctx, int nsteps, double eps);
+
+/* ---- host I/O (no GPU needed) ----------------------------------------- */
+/* Contents of the positional params file (sun.cpp:803-938).  Key names are
+ * read but not checked; the order is: header, NC, DIM, N0..N{DIM-1}, BETA, DT,
+ * STEPS, UPDATE, UPDATE2, CONFTAKE, LEVEL, VERBOSE, RUNCONTINUE, RANDOM, and,
+ * when RUNCONTINUE, TIME-STEP TAKEN NACC NAC1 NREC NTOT. */
+typedef struct {
+  int nc, dim, n[ASKJA_MAX_DIM];
+  double beta, dt;
+  int steps, update, update2, conftake, level, verbose, runcontinue, random;
+  int start, taken, nacc, nac1, nrec, ntot; /* resume trailer (START = TIME-STEP) */
+} askja_run_params;
+
+ASKJA_API int askja_params_load(const char* path, askja_run_params* out);
+/* store_parameters (sun.cpp:940-1057): copy `infile`'s key names with the
+ * run's values, RUNCONTINUE forced to 1, plus the TIME-STEP/TAKEN/NACC/NAC1/
+ * NREC/NTOT trailer. */
+ASKJA_API int askja_params_store(const char* infile, const char* outfile, const askja_run_params* p, int timestep, int taken);
+/* File stem "<dir>/<kind>-N%i-Nt%i-Ns%i-BETA%.2f-DT%.4f-U%.4f-CT%i" (sun.cpp:1124). */
+ASKJA_API int askja_file_stem(const askja_run_params* p, const char* dir, const char* kind, char* out, size_t cap);
+ASKJA_API int askja_conf_write(const char* path, const double* conf, long n_doubles); /* storeconf byte format */
+ASKJA_API int askja_conf_read(const char* path, double* conf, long n_doubles);        /* loadconf; short file = error */
+
+/* Pinned host memory for fast uploads (cudaMallocHost); NULL on failure. */
+ASKJA_API void* askja_host_alloc(size_t bytes);
+ASKJA_API void askja_host_free(void* p);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
