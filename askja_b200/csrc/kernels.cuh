@@ -79,12 +79,14 @@ template <int N, typename T>
 cudaError_t small_force(const LaunchCtx& c, int mode, const void* U, const void* Pin, void* Pout, void* Uout,
                         double ek, double ed) {
   using S2 = typename Storage<T>::type;
-  const unsigned grid = blocks_for(nlinks(c.lat), SMALL_THREADS);
+  // site tiles: 32 sites per CTA, one warp per direction (warps loop when DIM > 4)
+  const unsigned grid = blocks_for(c.lat.V, 32);
+  const int threads = 32 * std::min(c.lat.D, 4);
   if (mode == 0)
-    small::k_force<N, T, S2, 0><<<grid, SMALL_THREADS, 0, c.stream>>>(c.lat, (const S2*)U, (const S2*)Pin, (S2*)Pout,
+    small::k_force<N, T, S2, 0><<<grid, threads, 0, c.stream>>>(c.lat, (const S2*)U, (const S2*)Pin, (S2*)Pout,
                                                                       (S2*)Uout, (T)ek, (T)ed, c.order, c.reunit);
   else
-    small::k_force<N, T, S2, 1><<<grid, SMALL_THREADS, 0, c.stream>>>(c.lat, (const S2*)U, (const S2*)Pin, (S2*)Pout,
+    small::k_force<N, T, S2, 1><<<grid, threads, 0, c.stream>>>(c.lat, (const S2*)U, (const S2*)Pin, (S2*)Pout,
                                                                       (S2*)Uout, (T)ek, (T)ed, c.order, c.reunit);
   return cudaGetLastError();
 }

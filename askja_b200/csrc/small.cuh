@@ -262,14 +262,18 @@ __device__ __forceinline__ void reunitarise(Mat<N, T>& M) {
 
 // MODE 0: out-of-place kick        Pout = Pin - eps_k F(U)                (updateE)
 // MODE 1: fused kick + drift       P -= eps_k F(U); Uout = exp(i eps_d P) U
+//
+// Work mapping (site tiles): a CTA of 32*min(D,4) threads owns 32 consecutive
+// sites; warp w handles directions w, w+4, ... of those sites.  All D
+// directions of a site neighbourhood are therefore processed by one CTA at the
+// same time, so the neighbour links each staple needs are fetched from DRAM
+// once and then served from L1/L2 to the other warps, instead of being
+// re-fetched in D separate direction sweeps.  Each warp still reads 32
+// consecutive sites per element.
 template <int N, typename T, typename S2, int MODE>
-__global__ void __launch_bounds__(128) k_force(Lat L, const S2* __restrict__ U, const S2* Pin,
-                                               S2* Pout, S2* __restrict__ Uout, T eps_k, T eps_d,
-                                               int order, int reunit) {
-  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (long)L.V * L.D) return;
-  const int mu = (int)(t / L.V);
-  const int x = (int)(t - (long)mu * L.V);
+__device__ __forceinline__ void force_link(const Lat& L, const S2* __restrict__ U, const S2* Pin, S2* Pout,
+                                           S2* __restrict__ Uout, T eps_k, T eps_d, int order, int reunit, int mu,
+                                           int x) {
   Mat<N, T> acc, Ux, W;
   staple_sum<N, T, S2>(acc, U, L, mu, x);
   load(Ux, U, L, mu, x);
@@ -284,6 +288,16 @@ __global__ void __launch_bounds__(128) k_force(Lat L, const S2* __restrict__ U, 
     if (reunit) reunitarise(Tm);
     store(Uout, Tm, L, mu, x);
   }
+}
+
+template <int N, typename T, typename S2, int MODE>
+__global__ void __launch_bounds__(128) k_force(Lat L, const S2* __restrict__ U, const S2* Pin,
+                                               S2* Pout, S2* __restrict__ Uout, T eps_k, T eps_d,
+                                               int order, int reunit) {
+  const int x = blockIdx.x * 32 + (threadIdx.x & 31);
+  if (x >= L.V) return;
+  for (int mu = threadIdx.x >> 5; mu < L.D; mu += (blockDim.x >> 5)) force_link<N, T, S2, MODE>(
+      L, U, Pin, Pout, Uout, eps_k, eps_d, order, reunit, mu, x);
 }
 
 // In-place drift: U <- exp(i eps P) U (updateUandcopyDown; the copy pi = Pi is

@@ -1,0 +1,403 @@
+"""Benchmark: HMC link-updates/s on one B200 (or N independent replicas).
+
+Workload (default ``su3_32``): SU(3) Wilson action, DIM=4, lattice 32^4
+(1,048,576 sites, 4,194,304 links), BETA=6.0, DT=0.02, LEVEL=6, 50 leapfrog
+steps per trajectory, Haar-random hot start, seeded synthetic data.
+
+A bench "step" is one whole HMC trajectory on the device: momentum refresh,
+FP64 H_old, 50 fused kick+drift link updates, closing half kick, FP64 H_new,
+Metropolis and the accept/reject copy, replayed as one CUDA graph.
+``value`` = link updates per second over the timed trajectories
+(links x MD steps x trajectories / device time), aggregated over all ranks.
+The headline path is FP32-mixed (FP32 links, reunitarised, FP64 dH); the
+plain FP64 path is timed on the same workload and reported beside it.
+
+``e2e`` measures the same metric through the public C ABI with host buffers:
+every step uploads the configuration from pinned host memory
+(askja_set_links, U-conf layout FP64) and reads the trajectory result back.
+
+``--impl reference`` times the reference's own CPU code (sun.cpp's
+updateUandcopyDown + updateE, compiled from the reference sources against the
+project's GSL shim into oracle/_ref) on the host cores, one MD step of the
+same lattice per bench step; without that build it falls back to the
+project's C restatement (oracle/askja_oracle.c).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CONFIGS = {
+    # name: nc, dims, beta, dt, level, md steps per trajectory
+    "su3_32": dict(nc=3, dims=[32, 32, 32, 32], beta=6.0, dt=0.02, level=6, nsteps=50),
+    "su8_10": dict(nc=8, dims=[10, 10, 10, 10], beta=20.0, dt=0.01, level=8, nsteps=100),
+    "su3_8": dict(nc=3, dims=[8, 8, 8, 8], beta=5.70, dt=0.02, level=8, nsteps=50),
+}
+
+PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def peaks():
+    try:
+        with open(PEAKS_PATH) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region (every 200 ms)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        if self.path and os.path.exists(self.path):
+            for line in open(self.path):
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+            os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup(n_gpus: int):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def event_timer(stream_ptr: int, device: int):
+    import torch
+    s = torch.cuda.ExternalStream(stream_ptr, device=device)
+    return s, torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def time_trajectories(e, stream_ptr, device, nsteps, steps, warmup, world, clocks=None):
+    """W untimed trajectories, then K timed ones (graph replays) bracketed by
+    barrier + synchronize; CUDA events on the engine's stream."""
+    import torch
+    e.run_trajectories(warmup, nsteps, use_graph=True, want_log=False)
+    s, t0, t1 = event_timer(stream_ptr, device)
+    barrier(world)
+    torch.cuda.synchronize()
+    e.sync()
+    ctx = clocks if clocks is not None else _Null()
+    with ctx:
+        t0.record(s)
+        last, log = e.run_trajectories(steps, nsteps, use_graph=True, want_log=True)
+        t1.record(s)
+        t1.synchronize()
+    torch.cuda.synchronize()
+    barrier(world)
+    ms = t0.elapsed_time(t1)
+    return ms, last, log
+
+
+class _Null:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        return False
+
+
+def time_fused_kernel(e, stream_ptr, device, nlaunch, dt):
+    """Average duration of the fused kick+drift kernel: nlaunch back-to-back
+    launches (askja_leapfrog issues nlaunch fused launches + 1 kick)."""
+    s, t0, t1 = event_timer(stream_ptr, device)
+    e.leapfrog(2, dt)
+    e.sync()
+    t0.record(s)
+    e.leapfrog(nlaunch, dt)
+    t1.record(s)
+    t1.synchronize()
+    return t0.elapsed_time(t1) / (nlaunch + 1)
+
+
+def run_ours(args):
+    import torch
+
+    import askja_b200 as ab
+
+    world, rank, local = dist_setup(args.gpus)
+    cfg = CONFIGS[args.config]
+    nc, dims, nsteps = cfg["nc"], cfg["dims"], cfg["nsteps"]
+    vol = int(np.prod(dims))
+    links = vol * len(dims)
+    dev = local
+    torch.cuda.set_device(dev)
+    seed = 20240601 + 7919 * rank
+    res = {}
+    for prec in ("fp32", "fp64"):
+        with ab.Engine(nc, dims, beta=cfg["beta"], dt=cfg["dt"], level=cfg["level"], precision=prec, device=dev,
+                       seed=seed) as e:
+            e.hot_start(seed + 1)
+            K = args.steps if prec == "fp32" else max(3, args.steps // 2)
+            clocks = Clocks(dev) if prec == "fp32" else None
+            ms, last, log = time_trajectories(e, e.stream_ptr, dev, nsteps, K, args.warmup, world, clocks)
+            ms_max = max_over_ranks(ms, world)
+            lu = links * nsteps * K * world / (ms_max / 1e3)
+            r = dict(ms=ms_max, K=K, lu=lu, acc=last["n_acc"] / max(1, last["n_tot"]),
+                     dh_mean=float(np.mean(log[:, 2])), dh_abs=float(np.mean(np.abs(log[:, 2]))))
+            if clocks is not None:
+                r["clocks"] = clocks.summary()
+                # dominant kernel: fused kick+drift, timed alone
+                r["kernel_ms"] = time_fused_kernel(e, e.stream_ptr, dev, 20, cfg["dt"])
+                # e2e through the C ABI with host buffers
+                r.update(run_e2e(e, nsteps, max(3, K // 2), world))
+                t, s_ = e.PlaqExp()
+                r["plaq"] = 1.0 - (t + s_) / (vol * 6)
+            res[prec] = r
+    if rank != 0:
+        return None
+    f32, f64 = res["fp32"], res["fp64"]
+    hbm, peak_kind = peaks()
+    s = 8  # bytes per complex element, FP32
+    bytes_per_lu = 4 * nc * nc * s
+    achieved = bytes_per_lu * links / (f32["kernel_ms"] / 1e3) / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tp):
+        try:
+            traffic = json.load(open(tp)).get(f"{args.config}_fused_fp32_bytes_per_launch")
+        except Exception:
+            traffic = None
+    line = {
+        "metric": "link-updates/s (1 B200): FP32-mixed HMC trajectories, SU(3) 32^4",
+        "value": f32["lu"],
+        "unit": "link-updates/s",
+        "n_gpus": world,
+        "steps": f32["K"],
+        "warmup": args.warmup,
+        "ms_per_step": f32["ms"] / f32["K"],
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "fp32 (links, complex) / fp64 (dH, Metropolis)",
+        "data": "synthetic: seeded Haar hot start, Philox momenta",
+        "config": {"workload": f"{args.config}: SU({nc}) DIM={len(dims)} {'x'.join(map(str, dims))}, "
+                               f"BETA={cfg['beta']}, DT={cfg['dt']}, LEVEL={cfg['level']}, "
+                               f"{nsteps} MD steps/trajectory, 1 step = 1 trajectory",
+                   "links": links, "md_steps_per_traj": nsteps, "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (links 302 MB FP32 / 604 MB FP64)"},
+        "trajectories_per_s": world * f32["K"] / (f32["ms"] / 1e3),
+        "fp64": {"value": f64["lu"], "ms_per_step": f64["ms"] / f64["K"], "steps": f64["K"],
+                 "acceptance": f64["acc"], "mean_abs_dH": f64["dh_abs"]},
+        "mixed_over_fp64": f32["lu"] / f64["lu"],
+        "acceptance": f32["acc"],
+        "mean_abs_dH": f32["dh_abs"],
+        "plaquette": f32["plaq"],
+        "e2e": {"value": f32["e2e_lu"], "unit": "link-updates/s", "h2d_bytes_per_step": f32["h2d"],
+                "d2h_bytes_per_step": f32["d2h"]},
+        "roofline": {"bound": "hbm", "kernel": "fused kick+drift (small::k_force<3,float,1>)",
+                     "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "peak_source": peak_kind, "traffic": traffic,
+                     "bytes_per_launch": bytes_per_lu * links, "avg_launch_ms": f32["kernel_ms"]},
+        "gpu_launches": f32["K"] * (nsteps + 15) + f64["K"] * (nsteps + 15),
+        "clocks": f32["clocks"],
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(cfg, args.cpu_md_steps)
+    return line
+
+
+def run_e2e(e, nsteps, K, world):
+    """Same metric through the C ABI with host buffers: per trajectory, upload
+    the configuration from pinned host memory (FP64 U-conf layout) and read
+    the trajectory result back."""
+    import askja_b200 as ab
+    nbytes = int(np.prod(e.shape)) * 16
+    buf = ab.PinnedBuffer.alloc(nbytes)
+    try:
+        host = buf.array(np.complex128, e.shape)
+        host[...] = e.get_links()
+        e.trajectory(nsteps)  # warm (graphs not used on this path)
+        barrier(world)
+        t0 = time.perf_counter()
+        for _ in range(K):
+            e.set_links_ptr(buf.ptr)
+            e.trajectory(nsteps)
+        dt = time.perf_counter() - t0
+    finally:
+        buf.free()
+    dt = max_over_ranks(dt, world)
+    links = e.vol * e.dim
+    return {"e2e_lu": links * nsteps * K * world / dt, "h2d": nbytes, "d2h": 72}
+
+
+def cpu_baseline(cfg, md_steps):
+    """The reference's own CPU code on this host, one bounded sample."""
+    line = run_reference_sample(cfg, md_steps, warmup=0)
+    return line
+
+
+def run_reference_sample(cfg, steps, warmup):
+    from oracle import Reference, Oracle, fields
+    nc, dims = cfg["nc"], cfg["dims"]
+    cores = os.cpu_count() or 1
+    rng = np.random.default_rng(1)
+    vol = int(np.prod(dims))
+    links = vol * len(dims)
+    u = fields.haar(nc, links, rng).reshape(vol, len(dims), nc, nc)
+    O = Oracle(nc, dims)
+    p = fields.momenta(nc, links, cfg["beta"], rng, O)
+    if Reference.available():
+        R = Reference(nc, dims, beta=cfg["beta"], level=cfg["level"])
+        R.threads(cores)
+        R.set("u", u)
+        R.set("U", u)
+        R.set("pi", p)
+        R.set("Pi", p)
+        kind = "reference"
+
+        def step():
+            R.updateUandcopyDown(cfg["dt"])
+            R.updateE(cfg["dt"])
+    else:
+        kind = "port"
+        state = {"u": u, "p": p}
+
+        def step():
+            state["u"] = O.updateU(state["u"], state["p"], cfg["dt"], cfg["level"])
+            state["p"] = O.updateE(state["u"], state["p"], cfg["dt"])
+    for _ in range(warmup):
+        step()
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        step()
+        times.append(time.perf_counter() - t0)
+    per = float(np.mean(times))
+    return {"value": links / per, "unit": "link-updates/s", "cores": cores, "kind": kind,
+            "sample": f"{steps} MD step(s) (updateUandcopyDown + updateE) of SU({nc}) "
+                      f"{'x'.join(map(str, dims))}, OMP threads={cores}",
+            "seconds_per_md_step": per, "times": times}
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return None
+    cfg = CONFIGS[args.config]
+    r = run_reference_sample(cfg, args.steps, args.warmup)
+    nc, dims = cfg["nc"], cfg["dims"]
+    line = {
+        "impl": "reference",
+        "metric": "link-updates/s (1 B200): FP32-mixed HMC trajectories, SU(3) 32^4",
+        "value": r["value"], "unit": "link-updates/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": r["seconds_per_md_step"] * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp64", "data": "synthetic: seeded Haar links",
+        "config": {"workload": f"{args.config}: SU({nc}) DIM={len(dims)} {'x'.join(map(str, dims))}; "
+                               "1 step = 1 MD step of the reference CPU code", "parallelism": "CPU OpenMP"},
+        "cpu_baseline": {k: r[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "e2e": {"value": r["value"], "unit": "link-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    return line
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="su3_32", choices=sorted(CONFIGS))
+    ap.add_argument("--cpu-md-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        line = run_reference(args)
+    else:
+        line = run_ours(args)
+    if line is not None:
+        print(json.dumps(line), flush=True)
+    if int(os.environ.get("WORLD_SIZE", "1")) > 1 and args.impl == "ours":
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()
