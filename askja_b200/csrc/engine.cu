@@ -190,6 +190,10 @@ int download_conf(askja_ctx* c, const void* src, double* conf) {
 
 }  // namespace
 
+// Lets entry points without a context (static_plaq.cu) report through
+// askja_last_error(NULL).
+void askja_internal_set_error(const char* msg) { g_last_error = msg; }
+
 extern "C" {
 
 const char* askja_version(void) { return "askja-b200 0.1 (sm_100a)"; }

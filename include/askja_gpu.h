@@ -152,6 +152,30 @@ ASKJA_API int askja_leapfrog(askja_ctx* ctx, int nsteps, double eps);
  * reference's globals would. */
 ASKJA_API int askja_md_steps(askja_ctx* ctx, int nsteps, double eps);
 
+/* ---- allocation-free plaquette sums ------------------------------------ */
+/* No counterpart in the reference.  For callers that cannot let a library
+ * allocate GPU memory -- their device memory is owned by their own pool
+ * allocator, or they run on a fixed memory budget where a cudaMalloc would
+ * fail or synchronise the device mid-step.  Computes the same temporal and
+ * spatial plaquette sums as askja_PlaqExp (out[0] temporal, out[1] spatial,
+ * FP64) for a link field the caller already holds in device memory in this
+ * engine's layout (element (r,c) of link (site s, dir d) at
+ * ((d*NC + r)*NC + c)*V + s, double2 for ASKJA_FP64 or float2 for ASKJA_FP32
+ * per p->precision); `out` is device memory for 2 doubles.  Only p->nc,
+ * p->dim, p->n, p->precision and p->device are read.
+ *  - Allocates nothing: the per-block partial sums go to a fixed 128 KiB
+ *    static device array that every GPU loading the library keeps until exit.
+ *    Volumes above 2,097,152 sites are rejected with ASKJA_ERR_ARG.
+ *  - The first call on a device looks up that array's device address
+ *    (cudaGetSymbolAddress); make that first call before any stream capture.
+ *  - Work is enqueued on `stream` (NULL: the default stream) and the call
+ *    returns without waiting; `out` is valid once the stream reaches it.
+ *  - All calls share the one array (it keeps the last call's partials, each
+ *    call overwrites every slot it reads, nothing needs clearing), so calls
+ *    that overlap on the GPU race: serialise them on one stream.
+ *  - Errors are reported through askja_last_error(NULL). */
+ASKJA_API int askja_plaqexp_static(const askja_params* p, const void* links, double* out, void* stream);
+
 /* ---- host I/O (no GPU needed) ----------------------------------------- */
 /* Contents of the positional params file (sun.cpp:803-938).  Key names are
  * read but not checked; the order is: header, NC, DIM, N0..N{DIM-1}, BETA, DT,
