@@ -237,13 +237,7 @@ def run_ours(args):
     s = 8  # bytes per complex element, FP32
     bytes_per_lu = 4 * nc * nc * s
     achieved = bytes_per_lu * links / (f32["kernel_ms"] / 1e3) / 1e9
-    traffic = None
-    tp = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tp):
-        try:
-            traffic = json.load(open(tp)).get(f"{args.config}_fused_fp32_bytes_per_launch")
-        except Exception:
-            traffic = None
+    traffic = measured_traffic(args.config)
     line = {
         "metric": "link-updates/s (1 B200): FP32-mixed HMC trajectories, SU(3) 32^4",
         "value": f32["lu"],
@@ -281,6 +275,17 @@ def run_ours(args):
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(cfg, args.cpu_md_steps)
     return line
+
+
+def measured_traffic(config: str):
+    """DRAM bytes (read + write) per launch of the fused kernel from the
+    committed ncu summary of the same workload, or None."""
+    import re
+    path = os.path.join(ROOT, "profiles", "fused_kick_drift_su3_32x4.md")
+    if config != "su3_32" or not os.path.exists(path):
+        return None
+    m = re.search(r"traffic_bytes_per_launch_fp32_su3_32:\s*(\d+)", open(path).read())
+    return int(m.group(1)) if m else None
 
 
 def run_e2e(e, nsteps, K, world):
