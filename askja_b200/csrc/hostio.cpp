@@ -9,6 +9,7 @@
 #include <string.h>
 
 #include <fstream>
+#include <sstream>
 #include <string>
 
 #include "../../include/askja_gpu.h"
@@ -61,9 +62,15 @@ int askja_params_load(const char* path, askja_run_params* p) {
 
 int askja_params_store(const char* infile, const char* outfile, const askja_run_params* p, int timestep, int taken) {
   if (!infile || !outfile || !p) return ASKJA_ERR_ARG;
-  std::ifstream in(infile);
-  if (!in.is_open()) return ASKJA_ERR_IO;
-  std::string body;
+  // The input is read completely before the output is opened: on resume the
+  // master params file is both (the reference copies it to <infile>-tmp first,
+  // sun.cpp:945-949).
+  std::stringstream in;
+  {
+    std::ifstream fin(infile);
+    if (!fin.is_open()) return ASKJA_ERR_IO;
+    in << fin.rdbuf();
+  }
   {
     std::ofstream out(outfile, std::ios::out);
     if (!out.is_open()) return ASKJA_ERR_IO;
