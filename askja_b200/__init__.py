@@ -41,7 +41,7 @@ EXPORTS = [
     "askja_GaussLaw", "askja_UViol", "askja_WilsonLoop", "askja_PolyakovLoop", "askja_WilsonLoopDir",
     "askja_PlaqExp", "askja_scalarLoopcorr", "askja_trajectory", "askja_run_trajectories", "askja_leapfrog",
     "askja_md_steps", "askja_params_load", "askja_params_store", "askja_file_stem", "askja_conf_write",
-    "askja_conf_read", "askja_host_alloc", "askja_host_free", "askja_plaqexp_static",
+    "askja_conf_read", "askja_host_alloc", "askja_host_free", "askja_plaqexp_static", "askja_peak_flops",
 ]
 
 

@@ -1,14 +1,16 @@
 // Shared device-side building blocks for the askja B200 engine: complex
-// arithmetic on (re, im) pairs, the SoA field layout, the periodic neighbour
+// arithmetic on (re, im) pairs, the field layout, the periodic neighbour
 // table, Philox4x32-10 and Box-Muller.
 //
-// Field layout in HBM (all link and momentum fields):
-//   element (row r, col c) of the matrix on link (site s, direction d) lives at
-//   f[((d * NC + r) * NC + c) * V + s]  as float2 (FP32 mode) or double2 (FP64)
-// i.e. one plane of V complex numbers per (direction, matrix element).  A warp
-// that walks 32 consecutive sites of one direction therefore reads 32
-// consecutive complex numbers per element: 256 B (FP32) / 512 B (FP64) per
-// load instruction, fully coalesced.  Site numbering is the reference's
+// Field layout in HBM (all link and momentum fields), blocked by 32 sites:
+//   element e = r*NC + c of the matrix on link (site s, direction d) lives at
+//   f[((d * B + s/32) * NC*NC + e) * 32 + s%32],   B = ceil(V/32) site blocks,
+// as float2 (FP32 mode) or double2 (FP64 mode).  A warp that walks 32
+// consecutive sites of one direction reads 32 consecutive complex numbers per
+// element -- 256 B (FP32) / 512 B (FP64) per load instruction, coalesced --
+// and the NC*NC elements of one link are a fixed 32-element stride apart, so a
+// thread addresses a whole matrix from one base pointer with compile-time
+// offsets.  Sites V..32B-1 are padding.  Site numbering is the reference's
 // (structs.h:130-165): x0 slowest, x_{D-1} fastest.
 #pragma once
 
@@ -98,6 +100,7 @@ __device__ __forceinline__ void stc(S2* __restrict__ p, const cpx<T>& z) {
 // Geometry handed to every kernel by value.
 struct Lat {
   int V;           // sites
+  int B;           // 32-site blocks, ceil(V/32)
   int D;           // dimensions
   int N;           // colours
   const int* nbr;  // nbr[(2*d + 0)*V + s] = s + d^, nbr[(2*d + 1)*V + s] = s - d^
@@ -110,9 +113,19 @@ __device__ __forceinline__ int nb_minus(const Lat& L, int d, int s) {
   return __ldg(L.nbr + (size_t)(2 * d + 1) * L.V + s);
 }
 
-// Offset of element e of the link (d, s) in SoA layout.
-__device__ __forceinline__ size_t eoff(const Lat& L, int d, int e, int s) {
-  return ((size_t)d * L.N * L.N + e) * (size_t)L.V + s;
+// Offset of element 0 of the link (d, s); element e is at + 32*e.
+__host__ __device__ __forceinline__ size_t mbase(const Lat& L, int d, int s) {
+  return ((size_t)d * L.B + (s >> 5)) * (size_t)(L.N * L.N) * 32 + (s & 31);
+}
+
+// Offset of element e of the link (d, s).
+__host__ __device__ __forceinline__ size_t eoff(const Lat& L, int d, int e, int s) {
+  return mbase(L, d, s) + (size_t)e * 32;
+}
+
+// Complex elements in one field (padding included).
+__host__ __device__ __forceinline__ size_t field_elems(const Lat& L) {
+  return (size_t)L.D * L.B * 32 * L.N * L.N;
 }
 
 // ---- Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11) ----

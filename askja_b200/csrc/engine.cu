@@ -254,11 +254,12 @@ int askja_create(const askja_params* p, askja_ctx** out) {
   c->nl = V * p->dim;
   c->ks = p->precision == ASKJA_FP64 ? &askja::kernels_fp64 : &askja::kernels_fp32;
   const size_t elem = p->precision == ASKJA_FP64 ? 16 : 8;
-  c->field_bytes = (size_t)c->nl * c->N * c->N * elem;
   Lat& L = c->lat;
   L.V = (int)V;
+  L.B = (int)((V + 31) / 32);
   L.D = p->dim;
   L.N = p->nc;
+  c->field_bytes = askja::field_elems(L) * elem;
   for (int i = 0; i < p->dim; i++) {
     L.n[i] = p->n[i];
     long s = 1;

@@ -241,7 +241,7 @@ cudaError_t refresh(const LaunchCtx& c, void* P, uint64_t seed, const unsigned l
 template <typename T>
 cudaError_t identity(const LaunchCtx& c, void* U) {
   using S2 = typename Storage<T>::type;
-  const long tot = nlinks(c.lat) * c.lat.N * c.lat.N;
+  const long tot = (long)field_elems(c.lat);
   misc::k_identity<S2><<<blocks_for(tot, 256), 256, 0, c.stream>>>(c.lat, (S2*)U);
   return cudaGetLastError();
 }
@@ -256,7 +256,7 @@ cudaError_t gauss_matrices(const LaunchCtx& c, void* U, uint64_t seed) {
 template <typename T>
 cudaError_t from_conf(const LaunchCtx& c, const void* conf, void* f) {
   using S2 = typename Storage<T>::type;
-  const long tot = nlinks(c.lat) * c.lat.N * c.lat.N;
+  const long tot = (long)field_elems(c.lat);
   misc::k_from_conf<S2><<<blocks_for(tot, 256), 256, 0, c.stream>>>(c.lat, (const double2*)conf, (S2*)f);
   return cudaGetLastError();
 }

@@ -325,14 +325,13 @@ __global__ void k_refresh(Lat L, S2* __restrict__ P, uint64_t seed, const unsign
 }
 
 // Cold start (sun.cpp:194-207): every link the identity.
+// (Padding sites get the identity too.)
 template <typename S2>
 __global__ void k_identity(Lat L, S2* __restrict__ U) {
   const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long tot = (long)L.V * L.D * L.N * L.N;
-  if (t >= tot) return;
+  if (t >= (long)field_elems(L)) return;
   const int N = L.N;
-  const long plane = t / L.V;  // d*N*N + e
-  const int e = (int)(plane % (N * N));
+  const int e = (int)((t >> 5) % (N * N));
   const int i = e / N, j = e - i * N;
   stc(U + t, mkc<double>(i == j ? 1.0 : 0.0, 0.0));
 }
@@ -426,18 +425,22 @@ static __global__ void k_accept_copy(const TrajState* __restrict__ st, uint4* __
 }
 
 // Conversion between the host U-conf layout (FP64, [site][dir][row][col][re,im])
-// and the device SoA layout in either precision.
+// and the device layout in either precision.
 template <typename S2>
 __global__ void k_from_conf(Lat L, const double2* __restrict__ conf, S2* __restrict__ f) {
   const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long)field_elems(L)) return;
+  // t indexes the device field: t = ((d*B + b)*NN + e)*32 + lane, site = 32b + lane
   const int NN = L.N * L.N;
-  const long tot = (long)L.V * L.D * NN;
-  if (t >= tot) return;
-  // t indexes the SoA output: t = (d*NN + e)*V + s
-  const long plane = t / L.V;
-  const int s = (int)(t - plane * L.V);
-  const int d = (int)(plane / NN);
-  const int e = (int)(plane - (long)d * NN);
+  const long rest = t >> 5;
+  const int e = (int)(rest % NN);
+  const long db = rest / NN;
+  const int d = (int)(db / L.B);
+  const int s = (int)((db - (long)d * L.B) * 32 + (t & 31));
+  if (s >= L.V) {
+    stc(f + t, mkc<double>(0.0, 0.0));
+    return;
+  }
   const double2 v = conf[((size_t)s * L.D + d) * NN + e];
   stc(f + t, mkc<double>(v.x, v.y));
 }

@@ -24,22 +24,23 @@ struct Mat {
   cpx<T> a[N][N];
 };
 
+// one base address per matrix; the elements are 32 complex numbers apart
 template <int N, typename T, typename S2>
 __device__ __forceinline__ void load(Mat<N, T>& m, const S2* __restrict__ f, const Lat& L, int d, int s) {
-  const S2* p = f + (size_t)d * N * N * L.V + s;
+  const S2* p = f + ((size_t)d * L.B + (s >> 5)) * (N * N * 32) + (s & 31);
 #pragma unroll
   for (int i = 0; i < N; i++)
 #pragma unroll
-    for (int j = 0; j < N; j++) m.a[i][j] = ldc<T>(p + (size_t)(i * N + j) * L.V);
+    for (int j = 0; j < N; j++) m.a[i][j] = ldc<T>(p + (i * N + j) * 32);
 }
 
 template <int N, typename T, typename S2>
 __device__ __forceinline__ void store(S2* __restrict__ f, const Mat<N, T>& m, const Lat& L, int d, int s) {
-  S2* p = f + (size_t)d * N * N * L.V + s;
+  S2* p = f + ((size_t)d * L.B + (s >> 5)) * (N * N * 32) + (s & 31);
 #pragma unroll
   for (int i = 0; i < N; i++)
 #pragma unroll
-    for (int j = 0; j < N; j++) stc(p + (size_t)(i * N + j) * L.V, m.a[i][j]);
+    for (int j = 0; j < N; j++) stc(p + (i * N + j) * 32, m.a[i][j]);
 }
 
 template <int N, typename T>

@@ -47,6 +47,12 @@ __device__ __forceinline__ int step_site(const askja::Lat& L, int s, int d, int 
   return s + (nc - c) * L.stride[d];
 }
 
+// Offset of element e of link (d, s) in the plain SoA layout this entry point
+// takes: ((d*NC*NC + e)*V + s).
+__device__ __forceinline__ size_t soa(const askja::Lat& L, int d, int e, int s) {
+  return ((size_t)d * L.N * L.N + e) * (size_t)L.V + s;
+}
+
 // Same sums as askja::misc::k_plaq (temporal planes (0,k) / spatial planes
 // (j,k), j >= 1; FP64 accumulation), neighbours by arithmetic.
 template <typename S2>
@@ -66,10 +72,10 @@ __global__ void __launch_bounds__(kThreads) k_plaq_static(askja::Lat L, const S2
           for (int j = 0; j < N; j++) {
             cpx<double> ab = askja::czero<double>(), dc = askja::czero<double>();
             for (int k = 0; k < N; k++) {
-              askja::cmac(ab, askja::ldc<double>(U + askja::eoff(L, mu, i * N + k, s)),
-                          askja::ldc<double>(U + askja::eoff(L, nu, k * N + j, xpmu)));
-              askja::cmac(dc, askja::ldc<double>(U + askja::eoff(L, nu, i * N + k, s)),
-                          askja::ldc<double>(U + askja::eoff(L, mu, k * N + j, xpnu)));
+              askja::cmac(ab, askja::ldc<double>(U + soa(L, mu, i * N + k, s)),
+                          askja::ldc<double>(U + soa(L, nu, k * N + j, xpmu)));
+              askja::cmac(dc, askja::ldc<double>(U + soa(L, nu, i * N + k, s)),
+                          askja::ldc<double>(U + soa(L, mu, k * N + j, xpnu)));
             }
             tr += ab.re * dc.re + ab.im * dc.im;
           }

@@ -128,24 +128,28 @@ def barrier(world):
         dist.barrier()
 
 
-def max_over_ranks(x: float, world: int) -> float:
-    if world == 1:
-        return x
+def _all_reduce(x: float, op: str) -> float:
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
     return float(t.item())
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    """The slowest rank's time: the job is as fast as its slowest replica."""
+    return x if world == 1 else _all_reduce(x, "max")
 
 
 def sum_over_ranks(x: float, world: int) -> float:
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    return x if world == 1 else _all_reduce(x, "sum")
+
+
+def aggregate_rate(units_per_rank: float, world: int, seconds_max: float) -> float:
+    """Whole-job throughput: every rank processes `units_per_rank`, the job
+    takes the max over ranks of the device time."""
+    return units_per_rank * world / seconds_max
 
 
 def event_timer(stream_ptr: int, device: int):
@@ -218,7 +222,7 @@ def run_ours(args):
             clocks = Clocks(dev) if prec == "fp32" else None
             ms, last, log = time_trajectories(e, e.stream_ptr, dev, nsteps, K, args.warmup, world, clocks)
             ms_max = max_over_ranks(ms, world)
-            lu = links * nsteps * K * world / (ms_max / 1e3)
+            lu = aggregate_rate(links * nsteps * K, world, ms_max / 1e3)
             r = dict(ms=ms_max, K=K, lu=lu, acc=last["n_acc"] / max(1, last["n_tot"]),
                      dh_mean=float(np.mean(log[:, 2])), dh_abs=float(np.mean(np.abs(log[:, 2]))))
             if clocks is not None:
@@ -309,7 +313,7 @@ def run_e2e(e, nsteps, K, world):
         buf.free()
     dt = max_over_ranks(dt, world)
     links = e.vol * e.dim
-    return {"e2e_lu": links * nsteps * K * world / dt, "h2d": nbytes, "d2h": 72}
+    return {"e2e_lu": aggregate_rate(links * nsteps * K, world, dt), "h2d": nbytes, "d2h": 72}
 
 
 def cpu_baseline(cfg, md_steps):

@@ -158,8 +158,8 @@ ASKJA_API int askja_md_steps(askja_ctx* ctx, int nsteps, double eps);
  * allocator, or they run on a fixed memory budget where a cudaMalloc would
  * fail or synchronise the device mid-step.  Computes the same temporal and
  * spatial plaquette sums as askja_PlaqExp (out[0] temporal, out[1] spatial,
- * FP64) for a link field the caller already holds in device memory in this
- * engine's layout (element (r,c) of link (site s, dir d) at
+ * FP64) for a link field the caller already holds in device memory in plain
+ * structure-of-arrays order (element (r,c) of link (site s, dir d) at
  * ((d*NC + r)*NC + c)*V + s, double2 for ASKJA_FP64 or float2 for ASKJA_FP32
  * per p->precision); `out` is device memory for 2 doubles.  Only p->nc,
  * p->dim, p->n, p->precision and p->device are read.
@@ -175,6 +175,12 @@ ASKJA_API int askja_md_steps(askja_ctx* ctx, int nsteps, double eps);
  *    that overlap on the GPU race: serialise them on one stream.
  *  - Errors are reported through askja_last_error(NULL). */
 ASKJA_API int askja_plaqexp_static(const askja_params* p, const void* links, double* out, void* stream);
+
+/* ---- diagnostics (not in the reference) -------------------------------- */
+/* Measured compute-pipe peak of `device` for the roofline: which = 0 FP32
+ * FFMA, 1 FP32 packed FFMA2, 2 FP64 DFMA; GFLOP/s (2 flops per FMA lane),
+ * best of `repeats` launches.  Allocates a small scratch buffer. */
+ASKJA_API int askja_peak_flops(int device, int which, int repeats, double* gflops);
 
 /* ---- host I/O (no GPU needed) ----------------------------------------- */
 /* Contents of the positional params file (sun.cpp:803-938).  Key names are

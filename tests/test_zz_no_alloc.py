@@ -17,7 +17,7 @@ pytestmark = pytest.mark.gpu
 
 
 def _soa(u: np.ndarray, precision: str) -> np.ndarray:
-    """U-conf (V, D, N, N) -> the engine's device layout [d][r][c][site]."""
+    """U-conf (V, D, N, N) -> the plain structure-of-arrays order [d][r][c][site]."""
     a = np.ascontiguousarray(np.transpose(u, (1, 2, 3, 0)))
     return a.astype(np.complex64 if precision == "fp32" else np.complex128)
 
