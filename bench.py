@@ -276,9 +276,25 @@ def run_ours(args):
         "gpu_launches": f32["K"] * (nsteps + 15) + f64["K"] * (nsteps + 15),
         "clocks": f32["clocks"],
     }
+    if not args.no_precision:
+        line["precision"] = precision_report(cfg, dev)
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(cfg, args.cpu_md_steps)
     return line
+
+
+def precision_report(cfg, dev):
+    """FP32-mixed vs FP64 on identical (U, P) after a short FP32 thermalisation
+    from the hot start: force error, per-trajectory |dH32 - dH64|,
+    reversibility and unitarity (askja_b200.precision)."""
+    from askja_b200 import precision
+    nc, dims = cfg["nc"], cfg["dims"]
+    therm = 50
+    u0 = precision.thermalise(nc, dims, cfg["beta"], cfg["dt"], cfg["level"], cfg["nsteps"], therm, 4242, dev)
+    r = precision.compare(nc, dims, cfg["beta"], cfg["dt"], cfg["level"], cfg["nsteps"], u0, ntraj_dh=3,
+                          device=dev)
+    r["thermalisation_trajectories"] = therm
+    return r
 
 
 def measured_traffic(config: str):
@@ -396,6 +412,7 @@ def main():
     ap.add_argument("--config", default="su3_32", choices=sorted(CONFIGS))
     ap.add_argument("--cpu-md-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-precision", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         line = run_reference(args)

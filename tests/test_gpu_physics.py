@@ -194,3 +194,18 @@ def test_invalid_arguments():
             e.WilsonLoopDir(0)
         with pytest.raises(ab.AskjaError):
             e.trajectory(0)
+
+
+def test_precision_module_small():
+    """askja_b200.precision on a small lattice: FP32-mixed stays within
+    FP32-level distance of FP64 on identical inputs."""
+    from askja_b200 import precision
+    nc, dims, beta, dt, level, n = 3, [6, 6, 6, 6], 5.7, 0.02, 8, 10
+    u0 = precision.thermalise(nc, dims, beta, dt, level, n, 5, 3)
+    r = precision.compare(nc, dims, beta, dt, level, n, u0, ntraj_dh=2)
+    assert r["force_rel_err"] < 2e-5
+    assert r["max_abs_dH_diff"] < 5e-3
+    assert r["reversibility"]["fp64"] < 1e-10 and r["reversibility"]["fp32"] < 1e-5
+    assert r["unitarity_max"] < 5e-6
+    ens = precision.ensemble(nc, dims, beta, dt, level, n, u0, 10)
+    assert 0.3 < ens["fp64"]["plaquette"] < 0.7 and 0.3 < ens["fp32"]["plaquette"] < 0.7
