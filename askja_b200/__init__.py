@@ -42,6 +42,9 @@ EXPORTS = [
     "askja_PlaqExp", "askja_scalarLoopcorr", "askja_trajectory", "askja_run_trajectories", "askja_leapfrog",
     "askja_md_steps", "askja_params_load", "askja_params_store", "askja_file_stem", "askja_conf_write",
     "askja_conf_read", "askja_host_alloc", "askja_host_free", "askja_plaqexp_static", "askja_peak_flops",
+    "askja_batch_create", "askja_batch_destroy", "askja_batch_last_error", "askja_batch_stream",
+    "askja_batch_hot_start", "askja_batch_set_links", "askja_batch_get_links", "askja_batch_run",
+    "askja_batch_plaquette",
 ]
 
 
@@ -404,3 +407,99 @@ class PinnedBuffer:
         if self.ptr:
             library().askja_host_free(ctypes.c_void_p(self.ptr))
             self.ptr = 0
+
+
+class ChainParams(ctypes.Structure):
+    _fields_ = [("nc", ctypes.c_int), ("dim", ctypes.c_int), ("n", ctypes.c_int * MAX_DIM),
+                ("beta", ctypes.c_double), ("dt", ctypes.c_double), ("level", ctypes.c_int),
+                ("seed", ctypes.c_uint64)]
+
+
+class Batch:
+    """Many independent chains of uneven shape advanced together
+    (askja_batch_* of include/askja_gpu.h).  `chains` is a list of dicts with
+    keys nc, dims, beta, dt, level, seed."""
+
+    def __init__(self, chains, precision: str = "fp32", device: int = 0):
+        L = library()
+        vp = ctypes.c_void_p
+        L.askja_batch_create.argtypes = [ctypes.POINTER(ChainParams), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                         ctypes.POINTER(vp)]
+        L.askja_batch_destroy.argtypes = [vp]
+        L.askja_batch_destroy.restype = None
+        L.askja_batch_last_error.argtypes = [vp]
+        L.askja_batch_last_error.restype = ctypes.c_char_p
+        L.askja_batch_stream.argtypes = [vp]
+        L.askja_batch_stream.restype = vp
+        L.askja_batch_hot_start.argtypes = [vp, ctypes.c_uint64]
+        L.askja_batch_set_links.argtypes = [vp, ctypes.c_int, vp]
+        L.askja_batch_get_links.argtypes = [vp, ctypes.c_int, vp]
+        L.askja_batch_run.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(TrajResult)]
+        L.askja_batch_plaquette.argtypes = [vp, ctypes.POINTER(ctypes.c_double)]
+        self.lib = L
+        self.chains = [dict(c) for c in chains]
+        arr = (ChainParams * len(chains))()
+        for i, c in enumerate(self.chains):
+            arr[i].nc, arr[i].dim = int(c["nc"]), len(c["dims"])
+            for k, d in enumerate(c["dims"]):
+                arr[i].n[k] = int(d)
+            arr[i].beta, arr[i].dt = float(c["beta"]), float(c["dt"])
+            arr[i].level, arr[i].seed = int(c.get("level", 8)), int(c.get("seed", 1 + i))
+        self._b = ctypes.c_void_p()
+        rc = L.askja_batch_create(arr, len(chains), {"fp64": FP64, "fp32": FP32}[precision], int(device),
+                                  ctypes.byref(self._b))
+        if rc != ASKJA_OK:
+            raise AskjaError(rc, L.askja_batch_last_error(None).decode())
+
+    def _ck(self, rc):
+        if rc != ASKJA_OK:
+            raise AskjaError(rc, self.lib.askja_batch_last_error(self._b).decode())
+
+    def shape(self, c):
+        if not 0 <= c < len(self.chains):
+            raise AskjaError(-1, f"chain {c} out of range")
+        ch = self.chains[c]
+        return (int(np.prod(ch["dims"])), len(ch["dims"]), ch["nc"], ch["nc"])
+
+    def close(self):
+        if self._b:
+            self.lib.askja_batch_destroy(self._b)
+            self._b = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def stream_ptr(self) -> int:
+        return int(self.lib.askja_batch_stream(self._b) or 0)
+
+    def hot_start(self, seed: int):
+        self._ck(self.lib.askja_batch_hot_start(self._b, int(seed)))
+
+    def set_links(self, c: int, u):
+        u = np.ascontiguousarray(u, dtype=np.complex128).reshape(self.shape(c))
+        self._ck(self.lib.askja_batch_set_links(self._b, int(c), u.ctypes.data))
+
+    def get_links(self, c: int):
+        out = np.empty(self.shape(c), np.complex128)
+        self._ck(self.lib.askja_batch_get_links(self._b, int(c), out.ctypes.data))
+        return out
+
+    def run(self, ntraj: int, nsteps: int, use_graph: bool = True):
+        res = (TrajResult * len(self.chains))()
+        self._ck(self.lib.askja_batch_run(self._b, int(ntraj), int(nsteps), int(bool(use_graph)), res))
+        return [r.as_dict() for r in res]
+
+    def plaquette(self):
+        out = (ctypes.c_double * len(self.chains))()
+        self._ck(self.lib.askja_batch_plaquette(self._b, out))
+        return list(out)

@@ -28,9 +28,9 @@ CXX = "g++"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
                   "--expt-relaxed-constexpr", "-ccbin", CXX]
-CU_SOURCES = ["kernels_fp64.cu", "kernels_fp32.cu", "engine.cu", "static_plaq.cu", "peak.cu"]
+CU_SOURCES = ["kernels_fp64.cu", "kernels_fp32.cu", "engine.cu", "static_plaq.cu", "peak.cu", "batch.cu"]
 CPP_SOURCES = ["hostio.cpp"]
-HEADERS = ["common.cuh", "small.cuh", "rows.cuh", "misc.cuh", "kernels.cuh", "launch.h"]
+HEADERS = ["common.cuh", "small.cuh", "rows.cuh", "misc.cuh", "kernels.cuh", "launch.h", "batch.cuh"]
 
 
 def _newer(target: str, deps) -> bool:

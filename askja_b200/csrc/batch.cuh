@@ -1,0 +1,198 @@
+// Kernels that advance many independent Markov chains of uneven shape (NC,
+// DIM, extents, BETA, DT) together.  Every launch covers all chains (of one
+// colour number for the force) through a work list: work item i belongs to
+// the chain c with item_start[c] <= i < item_start[c+1]; the CTA copies that
+// chain's descriptor into shared memory and runs the same per-link / per-site
+// code as the single-chain kernels (small.cuh, rows.cuh, misc.cuh).  Chains
+// of different sizes therefore share the GPU in proportion to their work.
+#pragma once
+
+#include "misc.cuh"
+#include "rows.cuh"
+#include "small.cuh"
+
+namespace askja {
+namespace batch {
+
+struct ChainDev {
+  Lat lat;
+  void* U[2];
+  void* P;
+  void* Uconf;
+  double dt;
+  double beta;
+  double scale;  // sqrt(2 NC / beta)
+  int order;
+  int reunit;
+  uint64_t seed;
+  misc::TrajState* st;
+  double* sums;     // 8 doubles: [0,1] plaquette t/s, [2..4] link sums
+  double* partial;  // this chain's reduction partials
+  int plaq_blocks;  // RED_THREADS-site blocks
+  int link_blocks;  // RED_THREADS-link blocks
+  long n16;         // field size in 16-byte units
+};
+
+// chain owning work item i (item_start has nchains+1 entries, ascending)
+__device__ __forceinline__ int find_chain(const int* __restrict__ item_start, int nchains, int i) {
+  int lo = 0, hi = nchains - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(item_start + mid) <= i)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+// Copies the descriptor of the chain that owns this CTA's work item into
+// shared memory; returns the item's index within its chain.
+__device__ __forceinline__ int load_chain(ChainDev& sd, const ChainDev* __restrict__ descs,
+                                          const int* __restrict__ item_start, const int* __restrict__ chain_ids,
+                                          int nchains) {
+  __shared__ int s_local;
+  if (threadIdx.x == 0) {
+    const int k = find_chain(item_start, nchains, blockIdx.x);
+    const int c = chain_ids ? chain_ids[k] : k;
+    sd = descs[c];
+    s_local = blockIdx.x - item_start[k];
+  }
+  __syncthreads();
+  return s_local;
+}
+
+// Force (+ link update) for the small-NC chains of one colour number: item =
+// 32-site tile, 32*min(D,4) threads (see small::k_force).
+template <int N, typename T, int MODE>
+__global__ void __launch_bounds__(128) kb_force_small(const ChainDev* __restrict__ descs,
+                                                      const int* __restrict__ item_start,
+                                                      const int* __restrict__ chain_ids, int nchains, int cur,
+                                                      double kick_scale) {
+  using S2 = typename Storage<T>::type;
+  __shared__ ChainDev sd;
+  const int tile = load_chain(sd, descs, item_start, chain_ids, nchains);
+  const Lat& L = sd.lat;
+  const int x = tile * 32 + (threadIdx.x & 31);
+  if (x >= L.V) return;
+  const S2* U = (const S2*)sd.U[cur];
+  S2* P = (S2*)sd.P;
+  S2* Uo = (S2*)sd.U[cur ^ 1];
+  for (int mu = threadIdx.x >> 5; mu < L.D; mu += (blockDim.x >> 5))
+    small::force_link<N, T, S2, MODE>(L, U, P, P, Uo, (T)(kick_scale * sd.dt), (T)sd.dt, sd.order, sd.reunit, mu,
+                                      x);
+}
+
+// Same for the row-per-thread path: item = G links (G = blockDim / NC).
+template <int NMAX, typename T, int MODE>
+__global__ void kb_force_rows(const ChainDev* __restrict__ descs, const int* __restrict__ item_start,
+                              const int* __restrict__ chain_ids, int nchains, int cur, double kick_scale) {
+  using S2 = typename Storage<T>::type;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ int piv_s[64];
+  __shared__ cpx<T> det_s[64];
+  __shared__ ChainDev sd;
+  const int item = load_chain(sd, descs, item_start, chain_ids, nchains);
+  const int G = blockDim.x / sd.lat.N;
+  rows::force_rows<NMAX, T, S2, MODE>(sd.lat, (const S2*)sd.U[cur], (const S2*)sd.P, (S2*)sd.P,
+                                      (S2*)sd.U[cur ^ 1], (T)(kick_scale * sd.dt), (T)sd.dt, sd.order, sd.reunit,
+                                      (long)item * G, smem_raw, piv_s, det_s);
+}
+
+// Plaquette sums: item = RED_THREADS-site block; partial per chain block.
+template <typename S2>
+__global__ void __launch_bounds__(misc::RED_THREADS) kb_plaq(const ChainDev* __restrict__ descs,
+                                                             const int* __restrict__ item_start, int nchains,
+                                                             int cur) {
+  __shared__ ChainDev sd;
+  const int blk = load_chain(sd, descs, item_start, nullptr, nchains);
+  const S2* U = (const S2*)sd.U[cur];
+  const int s = blk * misc::RED_THREADS + threadIdx.x;
+  double v[2] = {0.0, 0.0};
+  switch (sd.lat.N) {
+    case 2: misc::plaq_site<2, S2>(sd.lat, U, s, v); break;
+    case 3: misc::plaq_site<3, S2>(sd.lat, U, s, v); break;
+    case 4: misc::plaq_site<4, S2>(sd.lat, U, s, v); break;
+    default: misc::plaq_site<0, S2>(sd.lat, U, s, v);
+  }
+  misc::block_sum<2>(v);
+  if (threadIdx.x == 0) {
+    sd.partial[2 * blk + 0] = v[0];
+    sd.partial[2 * blk + 1] = v[1];
+  }
+}
+
+// Kinetic sums sum tr2(P): item = RED_THREADS-link block.
+template <typename S2>
+__global__ void __launch_bounds__(misc::RED_THREADS) kb_kinetic(const ChainDev* __restrict__ descs,
+                                                                const int* __restrict__ item_start, int nchains) {
+  __shared__ ChainDev sd;
+  const int blk = load_chain(sd, descs, item_start, nullptr, nchains);
+  const long t = (long)blk * misc::RED_THREADS + threadIdx.x;
+  double v[3] = {0.0, 0.0, 0.0};
+  switch (sd.lat.N) {
+    case 2: misc::link_sums<2, S2>(sd.lat, (const S2*)sd.P, nullptr, nullptr, t, v); break;
+    case 3: misc::link_sums<3, S2>(sd.lat, (const S2*)sd.P, nullptr, nullptr, t, v); break;
+    case 4: misc::link_sums<4, S2>(sd.lat, (const S2*)sd.P, nullptr, nullptr, t, v); break;
+    default: misc::link_sums<0, S2>(sd.lat, (const S2*)sd.P, nullptr, nullptr, t, v);
+  }
+  misc::block_sum<3>(v);
+  // kinetic partials live after the plaquette partials
+  if (threadIdx.x == 0) sd.partial[2 * sd.plaq_blocks + blk] = v[0];
+}
+
+// One block per chain: sums its partials and, with `which` = 0 / 1, writes
+// H = beta (S + K / (2 NC)) to st->h_old / st->h_new.
+static __global__ void kb_energy(const ChainDev* __restrict__ descs, int which) {
+  const ChainDev& d = descs[blockIdx.x];
+  double v[3] = {0.0, 0.0, 0.0};
+  for (int b = threadIdx.x; b < d.plaq_blocks; b += blockDim.x) {
+    v[0] += d.partial[2 * b];
+    v[1] += d.partial[2 * b + 1];
+  }
+  for (int b = threadIdx.x; b < d.link_blocks; b += blockDim.x) v[2] += d.partial[2 * d.plaq_blocks + b];
+  misc::block_sum<3>(v);
+  if (threadIdx.x == 0) {
+    d.sums[0] = v[0];
+    d.sums[1] = v[1];
+    d.sums[2] = v[2];
+    const double h = d.beta * ((v[0] + v[1]) + v[2] / (2.0 * d.lat.N));
+    if (which == 0)
+      d.st->h_old = h;
+    else if (which == 1)
+      d.st->h_new = h;
+  }
+}
+
+static __global__ void kb_metropolis(const ChainDev* __restrict__ descs, int nchains) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < nchains) misc::metropolis(descs[c].st, descs[c].seed, nullptr, 0);
+}
+
+// Momentum refresh: item = 128-link block.
+template <typename S2>
+__global__ void __launch_bounds__(128) kb_refresh(const ChainDev* __restrict__ descs, const int* __restrict__ item_start,
+                                                  int nchains) {
+  __shared__ ChainDev sd;
+  const int blk = load_chain(sd, descs, item_start, nullptr, nchains);
+  misc::refresh_link<S2>(sd.lat, (S2*)sd.P, sd.seed, (uint32_t)sd.st->traj, sd.scale, (long)blk * 128 + threadIdx.x);
+}
+
+// Accept (uconf = u) or reject (u = uconf): item = 4096 x 16 bytes.
+static __global__ void __launch_bounds__(256) kb_accept_copy(const ChainDev* __restrict__ descs,
+                                                             const int* __restrict__ item_start, int nchains,
+                                                             int cur) {
+  __shared__ ChainDev sd;
+  const int blk = load_chain(sd, descs, item_start, nullptr, nchains);
+  const bool acc = sd.st->accepted != 0;
+  uint4* U = (uint4*)sd.U[cur];
+  uint4* C = (uint4*)sd.Uconf;
+  uint4* dst = acc ? C : U;
+  const uint4* src = acc ? U : C;
+  const long i0 = (long)blk * 4096;
+  const long i1 = min(sd.n16, i0 + 4096);
+  for (long i = i0 + threadIdx.x; i < i1; i += blockDim.x) dst[i] = src[i];
+}
+
+}  // namespace batch
+}  // namespace askja

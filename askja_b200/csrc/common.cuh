@@ -58,6 +58,19 @@ __device__ __forceinline__ void cmac(cpx<T>& acc, const cpx<T>& a, const cpx<T>&
   acc.im = fma(a.re, b.im, acc.im);
   acc.im = fma(a.im, b.re, acc.im);
 }
+// acc -= a * b
+template <typename T>
+__device__ __forceinline__ void cmsub(cpx<T>& acc, const cpx<T>& a, const cpx<T>& b) {
+  acc.re = fma(-a.re, b.re, acc.re);
+  acc.re = fma(a.im, b.im, acc.re);
+  acc.im = fma(-a.re, b.im, acc.im);
+  acc.im = fma(-a.im, b.re, acc.im);
+}
+// |a|^2 added to s
+template <typename T>
+__device__ __forceinline__ T cnorm2_add(const cpx<T>& a, T s) {
+  return fma(a.im, a.im, fma(a.re, a.re, s));
+}
 // acc += a * conj(b)
 template <typename T>
 __device__ __forceinline__ void cmac_nc(cpx<T>& acc, const cpx<T>& a, const cpx<T>& b) {

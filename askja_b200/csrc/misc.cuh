@@ -59,10 +59,8 @@ __global__ void k_finish(const double* __restrict__ partial, int nblocks, double
 // PlaqExp).  partial[b*2 + 0] = temporal planes (0,k), [b*2+1] = spatial (j,k), j>=1.
 // ReTr(A B C^dag D^dag) is evaluated as Re sum_ij (AB)_ij conj((DC)_ij).
 template <int NT, typename S2>
-__global__ void __launch_bounds__(RED_THREADS) k_plaq(Lat L, const S2* __restrict__ U, double* __restrict__ partial) {
+__device__ __forceinline__ void plaq_site(const Lat& L, const S2* __restrict__ U, int s, double (&v)[2]) {
   const int N = NT > 0 ? NT : L.N;
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  double v[2] = {0.0, 0.0};
   if (s < L.V) {
     for (int mu = 0; mu < L.D; mu++) {
       const int xpmu = nb_plus(L, mu, s);
@@ -79,12 +77,20 @@ __global__ void __launch_bounds__(RED_THREADS) k_plaq(Lat L, const S2* __restric
               cmac(ab, ldc<double>(U + eoff(L, mu, i * N + k, s)), ldc<double>(U + eoff(L, nu, k * N + j, xpmu)));
               cmac(dc, ldc<double>(U + eoff(L, nu, i * N + k, s)), ldc<double>(U + eoff(L, mu, k * N + j, xpnu)));
             }
-            tr += ab.re * dc.re + ab.im * dc.im;
+            // explicit fma: the same rounding in every kernel that inlines this
+            tr = fma(ab.re, dc.re, tr);
+            tr = fma(ab.im, dc.im, tr);
           }
         v[mu == 0 ? 0 : 1] += 1.0 - tr / N;
       }
     }
   }
+}
+
+template <int NT, typename S2>
+__global__ void __launch_bounds__(RED_THREADS) k_plaq(Lat L, const S2* __restrict__ U, double* __restrict__ partial) {
+  double v[2] = {0.0, 0.0};
+  plaq_site<NT, S2>(L, U, blockIdx.x * blockDim.x + threadIdx.x, v);
   block_sum<2>(v);
   if (threadIdx.x == 0) {
     partial[blockIdx.x * 2 + 0] = v[0];
@@ -96,11 +102,9 @@ __global__ void __launch_bounds__(RED_THREADS) k_plaq(Lat L, const S2* __restric
 // [1] = sum 1/4 ReTr((Pa+Pb)^2) (sun.cpp:560-567 EnergyEl, when Pb != null),
 // [2] = sum ReTr((U U^dag - 1)^2) (sun.cpp:441-471 UViol, when U != null).
 template <int NT, typename S2>
-__global__ void __launch_bounds__(RED_THREADS) k_linksums(Lat L, const S2* __restrict__ Pa, const S2* __restrict__ Pb,
-                                                          const S2* __restrict__ U, double* __restrict__ partial) {
+__device__ __forceinline__ void link_sums(const Lat& L, const S2* __restrict__ Pa, const S2* __restrict__ Pb,
+                                          const S2* __restrict__ U, long t, double (&v)[3]) {
   const int N = NT > 0 ? NT : L.N;
-  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  double v[3] = {0.0, 0.0, 0.0};
   if (t < (long)L.V * L.D) {
     const int d = (int)(t / L.V);
     const int s = (int)(t - (long)d * L.V);
@@ -112,11 +116,13 @@ __global__ void __launch_bounds__(RED_THREADS) k_linksums(Lat L, const S2* __res
         for (int j = 0; j < N; j++) {
           const cpx<double> x = ldc<double>(Pa + eoff(L, d, i * N + j, s));
           const cpx<double> y = ldc<double>(Pa + eoff(L, d, j * N + i, s));
-          a += x.re * y.re - x.im * y.im;
+          a = fma(x.re, y.re, a);
+          a = fma(-x.im, y.im, a);
           if (Pb) {
             const cpx<double> x2 = ldc<double>(Pb + eoff(L, d, i * N + j, s));
             const cpx<double> y2 = ldc<double>(Pb + eoff(L, d, j * N + i, s));
-            b += (x.re + x2.re) * (y.re + y2.re) - (x.im + x2.im) * (y.im + y2.im);
+            b = fma(x.re + x2.re, y.re + y2.re, b);
+            b = fma(-(x.im + x2.im), y.im + y2.im, b);
           }
         }
       v[0] = a;
@@ -138,11 +144,19 @@ __global__ void __launch_bounds__(RED_THREADS) k_linksums(Lat L, const S2* __res
             aij.re -= 1.0;
             aji.re -= 1.0;
           }
-          c += aij.re * aji.re - aij.im * aji.im;
+          c = fma(aij.re, aji.re, c);
+          c = fma(-aij.im, aji.im, c);
         }
       v[2] = c;
     }
   }
+}
+
+template <int NT, typename S2>
+__global__ void __launch_bounds__(RED_THREADS) k_linksums(Lat L, const S2* __restrict__ Pa, const S2* __restrict__ Pb,
+                                                          const S2* __restrict__ U, double* __restrict__ partial) {
+  double v[3] = {0.0, 0.0, 0.0};
+  link_sums<NT, S2>(L, Pa, Pb, U, (long)blockIdx.x * blockDim.x + threadIdx.x, v);
   block_sum<3>(v);
   if (threadIdx.x == 0)
 #pragma unroll
@@ -274,15 +288,13 @@ __global__ void __launch_bounds__(RED_THREADS) k_slice_trace(Lat L, const S2* __
 // generator is norm_m * diag(1,..,1 (m+1 times), -(m+1), 0, ..),
 // norm_m = sqrt(1 / (2 (m+1)(m+2))).
 template <typename S2>
-__global__ void k_refresh(Lat L, S2* __restrict__ P, uint64_t seed, const unsigned long long* __restrict__ traj_dev,
-                          unsigned long long traj_host, double scale) {
-  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void refresh_link(const Lat& L, S2* __restrict__ P, uint64_t seed, uint32_t traj,
+                                             double scale, long t) {
   if (t >= (long)L.V * L.D) return;
   const int N = L.N;
   const int d = (int)(t / L.V);
   const int s = (int)(t - (long)d * L.V);
   const unsigned long long lk = (unsigned long long)s * L.D + d;
-  const uint32_t traj = (uint32_t)(traj_dev ? *traj_dev : traj_host);
   const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
   int cur_blk = -1;
   double g[4];
@@ -322,6 +334,13 @@ __global__ void k_refresh(Lat L, S2* __restrict__ P, uint64_t seed, const unsign
     }
     stc(P + eoff(L, d, dd * N + dd, s), mkc<double>(scale * val, 0.0));
   }
+}
+
+template <typename S2>
+__global__ void k_refresh(Lat L, S2* __restrict__ P, uint64_t seed, const unsigned long long* __restrict__ traj_dev,
+                          unsigned long long traj_host, double scale) {
+  const uint32_t traj = (uint32_t)(traj_dev ? *traj_dev : traj_host);
+  refresh_link<S2>(L, P, seed, traj, scale, (long)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // Cold start (sun.cpp:194-207): every link the identity.
@@ -382,7 +401,7 @@ static __global__ void k_energy(const double* __restrict__ sums, double beta, in
   *h_out = beta * ((sums[0] + sums[1]) + sums[2] / (2.0 * N));
 }
 
-static __global__ void k_metropolis(TrajState* st, uint64_t seed, double* __restrict__ log_out, int log_cap) {
+__device__ __forceinline__ void metropolis(TrajState* st, uint64_t seed, double* __restrict__ log_out, int log_cap) {
   const double hn = st->h_new, ho = st->h_old;
   u32x4 c;
   c.x = 0xFFFFFFFFu;
@@ -411,6 +430,10 @@ static __global__ void k_metropolis(TrajState* st, uint64_t seed, double* __rest
     log_out[4 * k + 3] = (double)acc;
   }
   st->traj++;
+}
+
+static __global__ void k_metropolis(TrajState* st, uint64_t seed, double* __restrict__ log_out, int log_cap) {
+  metropolis(st, seed, log_out, log_cap);
 }
 
 // takeconfiguration / loadconfiguration (sun.cpp:725-742) after the test:

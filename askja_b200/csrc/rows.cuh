@@ -49,7 +49,7 @@ __device__ void reunitarise_tile(cpx<T>* S, cpx<T>* S2t, int N, int r, bool act,
   for (int q = 0; q < N; q++) {
     if (act && r == q) {
       T nrm = T(0);
-      for (int k = 0; k < N; k++) nrm += S[q * N + k].re * S[q * N + k].re + S[q * N + k].im * S[q * N + k].im;
+      for (int k = 0; k < N; k++) nrm = cnorm2_add(S[q * N + k], nrm);
       const T inv = T(1) / sqrt(nrm);
       for (int k = 0; k < N; k++) {
         S[q * N + k].re *= inv;
@@ -60,11 +60,7 @@ __device__ void reunitarise_tile(cpx<T>* S, cpx<T>* S2t, int N, int r, bool act,
     if (act && r > q) {
       cpx<T> pr = czero<T>();
       for (int k = 0; k < N; k++) cmac_cn(pr, S[q * N + k], S[r * N + k]);
-      for (int k = 0; k < N; k++) {
-        const cpx<T> b = S[q * N + k];
-        S[r * N + k].re -= pr.re * b.re - pr.im * b.im;
-        S[r * N + k].im -= pr.re * b.im + pr.im * b.re;
-      }
+      for (int k = 0; k < N; k++) cmsub(S[r * N + k], pr, S[q * N + k]);
     }
     __syncthreads();
   }
@@ -80,7 +76,7 @@ __device__ void reunitarise_tile(cpx<T>* S, cpx<T>* S2t, int N, int r, bool act,
       int piv = c;
       T best = T(-1);
       for (int i = c; i < N; i++) {
-        const T v = S2t[i * N + c].re * S2t[i * N + c].re + S2t[i * N + c].im * S2t[i * N + c].im;
+        const T v = cnorm2_add(S2t[i * N + c], T(0));
         if (v > best) {
           best = v;
           piv = i;
@@ -95,22 +91,19 @@ __device__ void reunitarise_tile(cpx<T>* S, cpx<T>* S2t, int N, int r, bool act,
         det_s->re = -det_s->re;
         det_s->im = -det_s->im;
       }
-      const cpx<T> p = S2t[c * N + c];
-      const cpx<T> d = *det_s;
-      *det_s = mkc<T>(d.re * p.re - d.im * p.im, d.re * p.im + d.im * p.re);
+      cpx<T> dp = czero<T>();
+      cmac(dp, *det_s, S2t[c * N + c]);
+      *det_s = dp;
       *piv_s = piv;
     }
     __syncthreads();
     if (act && r > c) {
       const cpx<T> p = S2t[c * N + c];
-      const T den = p.re * p.re + p.im * p.im;
-      const cpx<T> a = S2t[r * N + c];
-      const cpx<T> f = mkc<T>((a.re * p.re + a.im * p.im) / den, (a.im * p.re - a.re * p.im) / den);
-      for (int k = c; k < N; k++) {
-        const cpx<T> b = S2t[c * N + k];
-        S2t[r * N + k].re -= f.re * b.re - f.im * b.im;
-        S2t[r * N + k].im -= f.re * b.im + f.im * b.re;
-      }
+      const T den = cnorm2_add(p, T(0));
+      cpx<T> q = czero<T>();  // a conj(p)
+      cmac_nc(q, S2t[r * N + c], p);
+      const cpx<T> f = mkc<T>(q.re / den, q.im / den);
+      for (int k = c; k < N; k++) cmsub(S2t[r * N + k], f, S2t[c * N + k]);
     }
     __syncthreads();
   }
@@ -128,22 +121,23 @@ __device__ void reunitarise_tile(cpx<T>* S, cpx<T>* S2t, int N, int r, bool act,
 
 // MODE 0: out-of-place kick  Pout = Pin - eps_k F(U)
 // MODE 1: fused kick + drift P -= eps_k F(U); Uout = exp(i eps_d P) U
+// The CTA's groups take links link_base, link_base+1, ... in site-major order
+// (link = x*D + mu), so the groups of one CTA work on all directions of
+// neighbouring sites and share their neighbour links through L1/L2.
 template <int NMAX, typename T, typename S2, int MODE>
-__global__ void k_force(Lat L, const S2* __restrict__ U, const S2* Pin, S2* Pout,
-                        S2* __restrict__ Uout, T eps_k, T eps_d, int order, int reunit) {
+__device__ __forceinline__ void force_rows(const Lat& L, const S2* __restrict__ U, const S2* Pin, S2* Pout,
+                                           S2* __restrict__ Uout, T eps_k, T eps_d, int order, int reunit,
+                                           long link_base, unsigned char* smem_raw, int* piv_s, cpx<T>* det_s) {
   constexpr int KU = NMAX <= 16 ? NMAX : 1;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ int piv_s[64];
-  __shared__ cpx<T> det_s[64];
   const int N = L.N;
   const int G = blockDim.x / N;
   const int g = threadIdx.x / N;
   const int r = threadIdx.x - g * N;
   const bool in_group = g < G;
-  const long link = (long)blockIdx.x * G + g;
+  const long link = link_base + g;
   const bool act = in_group && link < (long)L.V * L.D;
-  const int mu = act ? (int)(link / L.V) : 0;
-  const int x = act ? (int)(link - (long)mu * L.V) : 0;
+  const int x = act ? (int)(link / L.D) : 0;
+  const int mu = act ? (int)(link - (long)x * L.D) : 0;
   cpx<T>* S0 = reinterpret_cast<cpx<T>*>(smem_raw) + (size_t)(in_group ? g : 0) * 2 * N * N;
   cpx<T>* S1 = S0 + N * N;
 
@@ -298,6 +292,16 @@ __global__ void k_force(Lat L, const S2* __restrict__ U, const S2* Pin, S2* Pout
     }
     if (act) store_row<NMAX, T, S2>(Uout, tm, L, mu, x, r);
   }
+}
+
+template <int NMAX, typename T, typename S2, int MODE>
+__global__ void k_force(Lat L, const S2* __restrict__ U, const S2* Pin, S2* Pout, S2* __restrict__ Uout, T eps_k,
+                        T eps_d, int order, int reunit) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ int piv_s[64];
+  __shared__ cpx<T> det_s[64];
+  force_rows<NMAX, T, S2, MODE>(L, U, Pin, Pout, Uout, eps_k, eps_d, order, reunit,
+                                (long)blockIdx.x * (blockDim.x / L.N), smem_raw, piv_s, det_s);
 }
 
 // In-place drift U <- exp(i eps P) U, optional reunitarisation.

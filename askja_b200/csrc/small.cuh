@@ -204,14 +204,11 @@ __device__ __forceinline__ void reunitarise(Mat<N, T>& M) {
 #pragma unroll
       for (int k = 0; k < N; k++) cmac_cn(pr, M.a[q][k], M.a[r][k]);
 #pragma unroll
-      for (int k = 0; k < N; k++) {
-        M.a[r][k].re -= pr.re * M.a[q][k].re - pr.im * M.a[q][k].im;
-        M.a[r][k].im -= pr.re * M.a[q][k].im + pr.im * M.a[q][k].re;
-      }
+      for (int k = 0; k < N; k++) cmsub(M.a[r][k], pr, M.a[q][k]);
     }
     T nrm = T(0);
 #pragma unroll
-    for (int k = 0; k < N; k++) nrm += M.a[r][k].re * M.a[r][k].re + M.a[r][k].im * M.a[r][k].im;
+    for (int k = 0; k < N; k++) nrm = cnorm2_add(M.a[r][k], nrm);
     const T inv = T(1) / sqrt(nrm);
 #pragma unroll
     for (int k = 0; k < N; k++) {
@@ -232,8 +229,7 @@ __device__ __forceinline__ void reunitarise(Mat<N, T>& M) {
       const int k1 = (k + 1) % 3, k2 = (k + 2) % 3;
       cpx<T> c = czero<T>();
       cmac(c, M.a[0][k1], M.a[1][k2]);
-      c.re -= M.a[0][k2].re * M.a[1][k1].re - M.a[0][k2].im * M.a[1][k1].im;
-      c.im -= M.a[0][k2].re * M.a[1][k1].im + M.a[0][k2].im * M.a[1][k1].re;
+      cmsub(c, M.a[0][k2], M.a[1][k1]);
       M.a[2][k] = mkc<T>(c.re, -c.im);
     }
   } else if (N == 4) {
@@ -251,8 +247,7 @@ __device__ __forceinline__ void reunitarise(Mat<N, T>& M) {
         const int q1 = (p + 1) % 3, q2 = (p + 2) % 3;
         cpx<T> t = czero<T>();
         cmac(t, M.a[1][cols[q1]], M.a[2][cols[q2]]);
-        t.re -= M.a[1][cols[q2]].re * M.a[2][cols[q1]].re - M.a[1][cols[q2]].im * M.a[2][cols[q1]].im;
-        t.im -= M.a[1][cols[q2]].re * M.a[2][cols[q1]].im + M.a[1][cols[q2]].im * M.a[2][cols[q1]].re;
+        cmsub(t, M.a[1][cols[q2]], M.a[2][cols[q1]]);
         cmac(m, M.a[0][cols[p]], t);
       }
       const T sgn = ((3 + k) & 1) ? T(-1) : T(1);

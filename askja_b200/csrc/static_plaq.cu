@@ -77,7 +77,8 @@ __global__ void __launch_bounds__(kThreads) k_plaq_static(askja::Lat L, const S2
               askja::cmac(dc, askja::ldc<double>(U + soa(L, nu, i * N + k, s)),
                           askja::ldc<double>(U + soa(L, mu, k * N + j, xpnu)));
             }
-            tr += ab.re * dc.re + ab.im * dc.im;
+            tr = fma(ab.re, dc.re, tr);
+            tr = fma(ab.im, dc.im, tr);
           }
         v[mu == 0 ? 0 : 1] += 1.0 - tr / N;
       }

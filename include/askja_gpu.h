@@ -152,6 +152,37 @@ ASKJA_API int askja_leapfrog(askja_ctx* ctx, int nsteps, double eps);
  * reference's globals would. */
 ASKJA_API int askja_md_steps(askja_ctx* ctx, int nsteps, double eps);
 
+/* ---- batched independent chains (not in the reference) ----------------- */
+/* Many independent HMC chains of uneven shape -- a beta scan, several colour
+ * numbers, dimensions and volumes -- advanced together: per MD step one force
+ * launch per colour number covers every chain of that colour number (the
+ * launches of different colour numbers run concurrently), the reductions,
+ * momentum refresh, Metropolis test and accept/reject copy are one launch
+ * each for all chains, and a whole trajectory of all chains is one CUDA graph.
+ * Each chain follows sun.cpp:1249-1318 with its own BETA, DT, LEVEL and seed. */
+typedef struct {
+  int nc, dim, n[ASKJA_MAX_DIM];
+  double beta, dt;
+  int level;
+  uint64_t seed;
+} askja_chain_params;
+
+typedef struct askja_batch askja_batch;
+
+ASKJA_API int askja_batch_create(const askja_chain_params* chains, int nchains, int precision, int device,
+                                 askja_batch** out);
+ASKJA_API void askja_batch_destroy(askja_batch* b);
+ASKJA_API const char* askja_batch_last_error(const askja_batch* b); /* b may be NULL: last create() error */
+ASKJA_API void* askja_batch_stream(askja_batch* b);
+ASKJA_API int askja_batch_hot_start(askja_batch* b, uint64_t seed); /* Haar SU(NC) links for every chain */
+ASKJA_API int askja_batch_set_links(askja_batch* b, int chain, const double* conf); /* U-conf layout */
+ASKJA_API int askja_batch_get_links(askja_batch* b, int chain, double* conf);
+/* ntraj trajectories of nsteps MD steps for all chains; results[c] (may be
+ * NULL) receives chain c's outcome of the last trajectory and its counters. */
+ASKJA_API int askja_batch_run(askja_batch* b, int ntraj, int nsteps, int use_graph, askja_traj_result* results);
+/* out[c] = mean plaquette 1 - EnergyMag / (V D (D-1)/2) of chain c */
+ASKJA_API int askja_batch_plaquette(askja_batch* b, double* out);
+
 /* ---- allocation-free plaquette sums ------------------------------------ */
 /* No counterpart in the reference.  For callers that cannot let a library
  * allocate GPU memory -- their device memory is owned by their own pool
