@@ -381,6 +381,99 @@ def run_reference_sample(cfg, steps, warmup):
             "seconds_per_md_step": per, "times": times}
 
 
+def batch_chains(n=64, seed=7):
+    """64 uneven chains: NC cycling over {2,3,4,8}, DIM over {2,3,4}, extents
+    16^2 .. 16^4 (incl. 4x16^3), BETA uniform over [2,4] * NC^2/3."""
+    rng = np.random.default_rng(seed)
+    shapes = {2: [[16, 16], [8, 16], [16, 8]], 3: [[16, 16, 16], [4, 16, 16], [8, 8, 8]],
+              4: [[16, 16, 16, 16], [4, 16, 16, 16], [8, 8, 8, 8], [4, 8, 8, 8]]}
+    chains = []
+    for i in range(n):
+        nc = (2, 3, 4, 8)[i % 4]
+        dim = (2, 3, 4)[(i // 4) % 3]
+        dims = shapes[dim][(i // 12) % len(shapes[dim])]
+        beta = float(rng.uniform(2.0, 4.0) * nc * nc / 3.0)
+        chains.append(dict(nc=nc, dims=list(dims), beta=beta, dt=0.1 / np.sqrt(beta), level=8, seed=1000 + i))
+    return chains
+
+
+def tune_dt(chains, nsteps, rounds=3, ntraj=6, dev=0):
+    """Adjust each chain's DT towards ~80 % acceptance (FP32 batch, untimed)."""
+    import askja_b200 as ab
+    for _ in range(rounds):
+        with ab.Batch(chains, precision="fp32", device=dev) as b:
+            b.hot_start(3)
+            b.run(4, nsteps)  # leave the hot-start transient
+            before = b.run(0, nsteps)
+            res = b.run(ntraj, nsteps)
+        for c, r, r0 in zip(chains, res, before):
+            acc = (r["n_acc"] - r0["n_acc"]) / max(1, r["n_tot"] - r0["n_tot"])
+            if acc < 0.65:
+                c["dt"] *= 0.75
+            elif acc > 0.92:
+                c["dt"] *= 1.25
+    return chains
+
+
+def run_batch(args):
+    """Config 'batch64': all chains in one batch (FP32-mixed) vs each chain
+    alone in FP64 through the single-chain engine."""
+    import torch
+
+    import askja_b200 as ab
+    dev = 0
+    torch.cuda.set_device(dev)
+    nsteps = 20
+    chains = tune_dt(batch_chains(), nsteps, dev=dev)
+    work = sum(int(np.prod(c["dims"])) * len(c["dims"]) for c in chains) * nsteps
+    with ab.Batch(chains, precision="fp32", device=dev) as b:
+        b.hot_start(5)
+        b.run(args.warmup, nsteps)
+        s, t0, t1 = event_timer(b.stream_ptr, dev)
+        torch.cuda.synchronize()
+        r0 = b.run(0, nsteps)
+        with Clocks(dev) as clocks:
+            t0.record(s)
+            res = b.run(args.steps, nsteps)
+            t1.record(s)
+            t1.synchronize()
+        ms = t0.elapsed_time(t1)
+        acc = [(r["n_acc"] - a["n_acc"]) / max(1, r["n_tot"] - a["n_tot"]) for r, a in zip(res, r0)]
+    batched = work * args.steps / (ms / 1e3)
+    # each chain alone (single-chain engine, CUDA graph), FP64 and FP32
+    alone = {}
+    for prec in ("fp64", "fp32"):
+        tot_ms = 0.0
+        for c in chains:
+            with ab.Engine(c["nc"], c["dims"], beta=c["beta"], dt=c["dt"], level=c["level"], precision=prec,
+                           device=dev, seed=c["seed"]) as e:
+                e.hot_start(5)
+                e.run_trajectories(2, nsteps, use_graph=True, want_log=False)
+                s, a, z = event_timer(e.stream_ptr, dev)
+                e.sync()
+                a.record(s)
+                e.run_trajectories(args.steps, nsteps, use_graph=True, want_log=False)
+                z.record(s)
+                z.synchronize()
+                tot_ms += a.elapsed_time(z)
+        alone[prec] = work * args.steps / (tot_ms / 1e3)
+    return {
+        "metric": "link-updates/s (1 B200): 64 uneven chains, FP32-mixed batched vs each chain alone in FP64",
+        "value": batched, "unit": "link-updates/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "fp32 (links) / fp64 (dH)", "data": "synthetic: Haar hot start, Philox momenta",
+        "config": {"workload": "batch64: NC in {2,3,4,8}, DIM in {2,3,4}, 16^2..16^4 incl. 4x16^3, "
+                               f"BETA in [2,4]*NC^2/3, {nsteps} MD steps/trajectory, DT tuned per chain, "
+                               "1 step = 1 trajectory of every chain",
+                   "chains": len(chains), "links_total": work // nsteps},
+        "alone_fp64": alone["fp64"], "alone_fp32": alone["fp32"],
+        "batched_over_alone_fp64": batched / alone["fp64"],
+        "batched_over_alone_fp32": batched / alone["fp32"],
+        "acceptance_mean": float(np.mean(acc)), "acceptance_min": float(np.min(acc)),
+        "clocks": clocks.summary(),
+    }
+
+
 def run_reference(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -409,13 +502,15 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="su3_32", choices=sorted(CONFIGS))
+    ap.add_argument("--config", default="su3_32", choices=sorted(CONFIGS) + ["batch64"])
     ap.add_argument("--cpu-md-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-precision", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         line = run_reference(args)
+    elif args.config == "batch64":
+        line = run_batch(args)
     else:
         line = run_ours(args)
     if line is not None:
