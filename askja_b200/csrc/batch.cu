@@ -136,7 +136,7 @@ cudaError_t launch_force(askja_batch* b, const askja_batch::Group& g, cudaStream
 #define ROWS(NM)                                                                                              \
   if (g.nmax == NM) {                                                                                         \
     auto k = mode ? kb_force_rows<NM, T, 1> : kb_force_rows<NM, T, 0>;                                        \
-    if (g.smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.smem); \
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.smem);                        \
     k<<<grid, blk, g.smem, st>>>(b->d_desc, g.d_start, g.d_ids, (int)g.chains.size(), b->cur, ks);          \
   }
   ROWS(8) ROWS(16) ROWS(32) ROWS(64)
@@ -358,8 +358,8 @@ int askja_batch_create(const askja_chain_params* chains, int nchains, int precis
       else
         askja::detail::Rows<float>::shape(N, &g.G, &g.smem);
       for (int c : g.chains) {
-        const long nl = (long)b->desc[c].lat.V * b->desc[c].lat.D;
-        start.push_back(start.back() + (int)((nl + g.G - 1) / g.G));
+        const Lat& L = b->desc[c].lat;
+        start.push_back(start.back() + (int)((L.V + g.G - 1) / g.G) * L.D);
       }
     }
     g.nitems = start.back();

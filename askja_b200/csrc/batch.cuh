@@ -83,7 +83,8 @@ __global__ void __launch_bounds__(128) kb_force_small(const ChainDev* __restrict
                                       x);
 }
 
-// Same for the row-per-thread path: item = G links (G = blockDim / NC).
+// Same for the row-per-thread path: item = G consecutive sites of one
+// direction (G = blockDim / NC), directions of a site block adjacent.
 template <int NMAX, typename T, int MODE>
 __global__ void kb_force_rows(const ChainDev* __restrict__ descs, const int* __restrict__ item_start,
                               const int* __restrict__ chain_ids, int nchains, int cur, double kick_scale) {
@@ -96,7 +97,7 @@ __global__ void kb_force_rows(const ChainDev* __restrict__ descs, const int* __r
   const int G = blockDim.x / sd.lat.N;
   rows::force_rows<NMAX, T, S2, MODE>(sd.lat, (const S2*)sd.U[cur], (const S2*)sd.P, (S2*)sd.P,
                                       (S2*)sd.U[cur ^ 1], (T)(kick_scale * sd.dt), (T)sd.dt, sd.order, sd.reunit,
-                                      (long)item * G, smem_raw, piv_s, det_s);
+                                      item % sd.lat.D, (item / sd.lat.D) * G, smem_raw, piv_s, det_s);
 }
 
 // Plaquette sums: item = RED_THREADS-site block; partial per chain block.

@@ -32,10 +32,12 @@ struct Rows {
   }
 };
 
+// Opt in to the dynamic shared memory a launch needs (the kernels also have
+// static shared arrays, so the 48 KB default can be exceeded below 48 KB of
+// dynamic memory).
 template <typename Kern>
 cudaError_t set_smem(Kern k, size_t smem) {
-  if (smem > 48 * 1024) return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  return cudaSuccess;
+  return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
 template <int NMAX, typename T>
@@ -45,7 +47,8 @@ cudaError_t rows_force(const LaunchCtx& c, int mode, const void* U, const void* 
   int G;
   size_t smem;
   Rows<T>::shape(c.lat.N, &G, &smem);
-  const unsigned grid = blocks_for(nlinks(c.lat), G);
+  // G consecutive sites of one direction per CTA, all directions of a site block adjacent
+  const unsigned grid = blocks_for(c.lat.V, G) * c.lat.D;
   cudaError_t e;
   if (mode == 0) {
     auto k = rows::k_force<NMAX, T, S2, 0>;

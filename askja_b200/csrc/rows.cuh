@@ -1,12 +1,14 @@
 // Row-per-thread kernels for medium colour number (5 <= NC <= NMAX): a group
 // of NC threads owns one link, thread r owns row r of every matrix of the
-// staple sum in registers.  Products whose right operand is a stored link read
-// it straight from global memory (all NC threads of a group read the same
-// element in the same instruction, so L1 serves it as a broadcast); only
-// products whose right operand is itself a computed matrix (U_mu * staple sum,
-// the Horner recursion, Gram-Schmidt) stage it through a per-group tile of
-// shared memory.  Groups of one CTA are lock-stepped by __syncthreads, so every
-// thread, valid or not, runs the same barrier sequence.
+// staple sum in registers.  Every operand of a product -- a stored neighbour
+// link or a computed matrix (U_mu * staple sum, the Horner recursion,
+// Gram-Schmidt) -- goes through a per-group shared-memory tile; stored links
+// are copied in by the whole CTA with coalesced loads (see force_rows), and
+// the products read the tiles two complex numbers per load.  Groups of one CTA
+// are lock-stepped by __syncthreads, so every
+// thread, valid or not, runs the same barrier sequence.  Loops over matrix
+// indices are fully unrolled with predicated bodies (no early exits) so the
+// row arrays stay in registers.
 //
 // Same physics and conventions as small.cuh (sun.cpp:672-790, sunmat.h).
 #pragma once
@@ -16,10 +18,121 @@
 namespace askja {
 namespace rows {
 
-// shared memory per group: two NC x NC tiles
+// shared memory per group: three NC x NP staging tiles, NP = NC rounded up to
+// even so that every row starts on a 16-byte boundary, plus 16 bytes of skew
+// so that the groups of one warp start in different banks (without it the
+// tiles are a multiple of 128 bytes apart and every load is a bank conflict)
+template <typename T>
+__host__ __device__ inline size_t group_elems(int N) {
+  return 3 * (size_t)N * (N + (N & 1)) + 16 / sizeof(cpx<T>);
+}
 template <typename T>
 __host__ __device__ inline size_t smem_per_group(int N) {
-  return 2 * (size_t)N * N * sizeof(cpx<T>);
+  return group_elems<T>(N) * sizeof(cpx<T>);
+}
+template <typename T>
+__device__ __forceinline__ cpx<T>* group_tile(unsigned char* smem_raw, int g, int N) {
+  return reinterpret_cast<cpx<T>*>(smem_raw) + (size_t)g * group_elems<T>(N);
+}
+
+// tile[r*NP + c] = element (r, c) of the link (d, s), for c < NC; elements are
+// written in pairs (one 16-byte store in FP32; the odd padding column of an
+// odd NC gets a zero)
+template <int NMAX, typename T, typename S2>
+__device__ __forceinline__ void stage_row(cpx<T>* tile, int NP, const S2* __restrict__ f, const Lat& L, int d,
+                                          int s, int r) {
+  const int N = L.N;
+  const S2* p = f + mbase(L, d, s) + (size_t)r * N * 32;
+#pragma unroll
+  for (int c = 0; c < NMAX; c += 2) {
+    if (c >= N) continue;
+    const cpx<T> v0 = ldc<T>(p + c * 32);
+    const cpx<T> v1 = c + 1 < N ? ldc<T>(p + (c + 1) * 32) : czero<T>();
+    if constexpr (sizeof(T) == 4) {
+      *reinterpret_cast<float4*>(tile + r * NP + c) = make_float4(v0.re, v0.im, v1.re, v1.im);
+    } else {
+      tile[r * NP + c] = v0;
+      tile[r * NP + c + 1] = v1;
+    }
+  }
+}
+
+// two consecutive complex numbers from shared memory (16-byte load in FP32)
+template <typename T>
+__device__ __forceinline__ void ld2(const cpx<T>* p, cpx<T>& a, cpx<T>& b) {
+  if constexpr (sizeof(T) == 4) {
+    const float4 v = *reinterpret_cast<const float4*>(p);
+    a = mkc<T>(v.x, v.y);
+    b = mkc<T>(v.z, v.w);
+  } else {
+    a = p[0];
+    b = p[1];
+  }
+}
+
+// t[c] = sum_k A_k conj(tile[c][k]),  A_k = conj(a[k]) when CONJ_A else a[k]
+template <int NMAX, typename T, bool CONJ_A>
+__device__ __forceinline__ void row_times_tile_dag(cpx<T> (&t)[NMAX], const cpx<T> (&a)[NMAX], const cpx<T>* tile,
+                                                   int NP, int N) {
+  constexpr int KU = NMAX <= 16 ? NMAX : 1;
+#pragma unroll KU
+  for (int c = 0; c < NMAX; c++) {
+    if (c >= N) continue;
+    cpx<T> s = czero<T>();
+#pragma unroll KU
+    for (int k = 0; k < NMAX; k += 2) {
+      if (k >= N) continue;
+      cpx<T> b0, b1;
+      ld2(tile + c * NP + k, b0, b1);
+      if (CONJ_A) {
+        cmac_cc(s, a[k], b0);
+        if (k + 1 < N) cmac_cc(s, a[k + 1], b1);
+      } else {
+        cmac_nc(s, a[k], b0);
+        if (k + 1 < N) cmac_nc(s, a[k + 1], b1);
+      }
+    }
+    t[c] = s;
+  }
+}
+
+// acc[c] += sum_k t[k] conj(tile[c][k])
+template <int NMAX, typename T>
+__device__ __forceinline__ void row_times_tile_dag_acc(cpx<T> (&acc)[NMAX], const cpx<T> (&t)[NMAX],
+                                                       const cpx<T>* tile, int NP, int N) {
+  constexpr int KU = NMAX <= 16 ? NMAX : 1;
+#pragma unroll KU
+  for (int c = 0; c < NMAX; c++) {
+    if (c >= N) continue;
+#pragma unroll KU
+    for (int k = 0; k < NMAX; k += 2) {
+      if (k >= N) continue;
+      cpx<T> b0, b1;
+      ld2(tile + c * NP + k, b0, b1);
+      cmac_nc(acc[c], t[k], b0);
+      if (k + 1 < N) cmac_nc(acc[c], t[k + 1], b1);
+    }
+  }
+}
+
+// acc[c] += sum_k t[k] tile[k][c]
+template <int NMAX, typename T>
+__device__ __forceinline__ void row_times_tile_acc(cpx<T> (&acc)[NMAX], const cpx<T> (&t)[NMAX], const cpx<T>* tile,
+                                                   int NP, int N) {
+  constexpr int KU = NMAX <= 16 ? NMAX : 1;
+#pragma unroll KU
+  for (int k = 0; k < NMAX; k++) {
+    if (k >= N) continue;
+    const cpx<T> tk = t[k];
+#pragma unroll KU
+    for (int c = 0; c < NMAX; c += 2) {
+      if (c >= N) continue;
+      cpx<T> b0, b1;
+      ld2(tile + k * NP + c, b0, b1);
+      cmac(acc[c], tk, b0);
+      if (c + 1 < N) cmac(acc[c + 1], tk, b1);
+    }
+  }
 }
 
 template <int NMAX, typename T, typename S2>
@@ -112,8 +225,9 @@ __device__ void reunitarise_tile(cpx<T>* S, cpx<T>* S2t, int N, int r, bool act,
     const T dn = sqrt(d.re * d.re + d.im * d.im);
     const cpx<T> cph = mkc<T>(d.re / dn, -d.im / dn);
     for (int k = 0; k < N; k++) {
-      const cpx<T> x = S[r * N + k];
-      S[r * N + k] = mkc<T>(x.re * cph.re - x.im * cph.im, x.re * cph.im + x.im * cph.re);
+      cpx<T> y = czero<T>();
+      cmac(y, S[r * N + k], cph);
+      S[r * N + k] = y;
     }
   }
   __syncthreads();
@@ -121,110 +235,122 @@ __device__ void reunitarise_tile(cpx<T>* S, cpx<T>* S2t, int N, int r, bool act,
 
 // MODE 0: out-of-place kick  Pout = Pin - eps_k F(U)
 // MODE 1: fused kick + drift P -= eps_k F(U); Uout = exp(i eps_d P) U
-// The CTA's groups take links link_base, link_base+1, ... in site-major order
-// (link = x*D + mu), so the groups of one CTA work on all directions of
-// neighbouring sites and share their neighbour links through L1/L2.
+//
+// A CTA owns GS = blockDim/NC consecutive sites site0 .. site0+GS-1 of one
+// direction mu; group g (NC threads) computes the link (site0+g, mu), thread r
+// of the group owns row r.  Every matrix a group needs is copied into its
+// shared-memory tile by the whole CTA in "copy role": thread t copies row
+// t / GS of group t % GS, so consecutive threads read the same element of
+// consecutive sites -- coalesced, in the 32-site blocked field layout -- and
+// the compute role then reads rows and columns from the tiles.  Outputs (P and
+// the new links) go back the same way.
 template <int NMAX, typename T, typename S2, int MODE>
 __device__ __forceinline__ void force_rows(const Lat& L, const S2* __restrict__ U, const S2* Pin, S2* Pout,
-                                           S2* __restrict__ Uout, T eps_k, T eps_d, int order, int reunit,
-                                           long link_base, unsigned char* smem_raw, int* piv_s, cpx<T>* det_s) {
-  constexpr int KU = NMAX <= 16 ? NMAX : 1;
+                                           S2* __restrict__ Uout, T eps_k, T eps_d, int order, int reunit, int mu,
+                                           int site0, unsigned char* smem_raw, int* piv_s, cpx<T>* det_s) {
   const int N = L.N;
-  const int G = blockDim.x / N;
-  const int g = threadIdx.x / N;
-  const int r = threadIdx.x - g * N;
-  const bool in_group = g < G;
-  const long link = link_base + g;
-  const bool act = in_group && link < (long)L.V * L.D;
-  const int x = act ? (int)(link / L.D) : 0;
-  const int mu = act ? (int)(link - (long)x * L.D) : 0;
-  cpx<T>* S0 = reinterpret_cast<cpx<T>*>(smem_raw) + (size_t)(in_group ? g : 0) * 2 * N * N;
-  cpx<T>* S1 = S0 + N * N;
+  const int NP = N + (N & 1);
+  const int GS = blockDim.x / N;
+  const int tid = threadIdx.x;
+  // compute role
+  const int g = tid / N;
+  const int r = tid - g * N;
+  const bool act = g < GS && site0 + g < L.V;
+  cpx<T>* T0 = group_tile<T>(smem_raw, act ? g : 0, N);
+  cpx<T>* T1 = T0 + N * NP;
+  cpx<T>* T2 = T1 + N * NP;
+  // copy role
+  const int cg = tid % GS;
+  const int cr = tid / GS;
+  const int cx = site0 + cg;
+  const bool cact = cr < N && cx < L.V;
+  cpx<T>* C0 = group_tile<T>(smem_raw, cg, N);
+  cpx<T>* C1 = C0 + N * NP;
+  cpx<T>* C2 = C1 + N * NP;
 
-  cpx<T> acc[NMAX];
+  cpx<T> acc[NMAX], a[NMAX], t[NMAX];
 #pragma unroll
   for (int c = 0; c < NMAX; c++) acc[c] = czero<T>();
 
-  if (act) {
-    const int xpmu = nb_plus(L, mu, x);
-    for (int nu = 0; nu < L.D; nu++) {
-      if (nu == mu) continue;
-      const int xpnu = nb_plus(L, nu, x);
-      const int xmnu = nb_minus(L, nu, x);
-      const int xpmu_mnu = nb_minus(L, nu, xpmu);
-      cpx<T> t[NMAX];
-      // upper: t = row r of U_nu(x+mu) U_mu^dag(x+nu)
+  const int cxpmu = cact ? nb_plus(L, mu, cx) : 0;
+  for (int j = 0; j < L.D - 1; j++) {
+    const int nu = j < mu ? j : j + 1;
+    // upper: t = row r of U_nu(x+mu) U_mu^dag(x+nu); acc += t U_nu^dag(x)
+    __syncthreads();
+    if (cact) {
+      stage_row<NMAX, T, S2>(C0, NP, U, L, mu, nb_plus(L, nu, cx), cr);
+      stage_row<NMAX, T, S2>(C1, NP, U, L, nu, cx, cr);
+      stage_row<NMAX, T, S2>(C2, NP, U, L, nu, cxpmu, cr);
+    }
+    __syncthreads();
+    if (act) {
 #pragma unroll
-      for (int c = 0; c < NMAX; c++) t[c] = czero<T>();
-      for (int k = 0; k < N; k++) {
-        const cpx<T> a = ldc<T>(U + eoff(L, nu, r * N + k, xpmu));
+      for (int k = 0; k < NMAX; k++)
+        if (k < N) a[k] = T2[r * NP + k];
+      row_times_tile_dag<NMAX, T, false>(t, a, T0, NP, N);
+      row_times_tile_dag_acc<NMAX, T>(acc, t, T1, NP, N);
+    }
+    // lower: t = row r of U_nu^dag(x+mu-nu) U_mu^dag(x-nu); acc += t U_nu(x-nu)
+    __syncthreads();
+    if (cact) {
+      const int cxmnu = nb_minus(L, nu, cx);
+      stage_row<NMAX, T, S2>(C0, NP, U, L, nu, nb_minus(L, nu, cxpmu), cr);
+      stage_row<NMAX, T, S2>(C1, NP, U, L, mu, cxmnu, cr);
+      stage_row<NMAX, T, S2>(C2, NP, U, L, nu, cxmnu, cr);
+    }
+    __syncthreads();
+    if (act) {
 #pragma unroll
-        for (int c = 0; c < NMAX; c++)
-          if (c < N) cmac_nc(t[c], a, ldc<T>(U + eoff(L, mu, c * N + k, xpnu)));
-      }
-      // acc += t U_nu^dag(x)
-#pragma unroll KU
-      for (int k = 0; k < NMAX; k++) {
-        if (k >= N) break;
-        const cpx<T> tk = t[k];
-#pragma unroll
-        for (int c = 0; c < NMAX; c++)
-          if (c < N) cmac_nc(acc[c], tk, ldc<T>(U + eoff(L, nu, c * N + k, x)));
-      }
-      // lower: t = row r of U_nu^dag(x+mu-nu) U_mu^dag(x-nu)
-#pragma unroll
-      for (int c = 0; c < NMAX; c++) t[c] = czero<T>();
-      for (int k = 0; k < N; k++) {
-        const cpx<T> a = ldc<T>(U + eoff(L, nu, k * N + r, xpmu_mnu));  // (A^dag)[r][k] = conj(A[k][r])
-#pragma unroll
-        for (int c = 0; c < NMAX; c++)
-          if (c < N) cmac_cc(t[c], a, ldc<T>(U + eoff(L, mu, c * N + k, xmnu)));
-      }
-      // acc += t U_nu(x-nu)
-#pragma unroll KU
-      for (int k = 0; k < NMAX; k++) {
-        if (k >= N) break;
-        const cpx<T> tk = t[k];
-#pragma unroll
-        for (int c = 0; c < NMAX; c++)
-          if (c < N) cmac(acc[c], tk, ldc<T>(U + eoff(L, nu, k * N + c, xmnu)));
-      }
+      for (int k = 0; k < NMAX; k++)
+        if (k < N) a[k] = T0[k * NP + r];  // column r: row r of the adjoint, conjugated below
+      row_times_tile_dag<NMAX, T, true>(t, a, T1, NP, N);
+      row_times_tile_acc<NMAX, T>(acc, t, T2, NP, N);
     }
   }
-  // W = U_mu(x) * acc  (acc staged through S0)
+  // U_mu(x) -> T2 (rows kept in u[]), P(x) -> T1 (rows kept in p[])
+  cpx<T> u[NMAX], p[NMAX];
+  __syncthreads();
+  if (cact) {
+    stage_row<NMAX, T, S2>(C2, NP, U, L, mu, cx, cr);
+    stage_row<NMAX, T, S2>(C1, NP, Pin, L, mu, cx, cr);
+  }
+  __syncthreads();
   if (act) {
 #pragma unroll
     for (int c = 0; c < NMAX; c++)
-      if (c < N) S0[r * N + c] = acc[c];
+      if (c < N) {
+        u[c] = T2[r * NP + c];
+        p[c] = T1[r * NP + c];
+      }
+  }
+  __syncthreads();
+  // W = U_mu(x) acc: acc rows -> T0, w[c] = sum_k u[k] acc[k][c]; W rows -> T1
+  if (act) {
+#pragma unroll
+    for (int c = 0; c < NMAX; c++)
+      if (c < N) T0[r * NP + c] = acc[c];
   }
   __syncthreads();
   cpx<T> w[NMAX];
 #pragma unroll
   for (int c = 0; c < NMAX; c++) w[c] = czero<T>();
   if (act) {
-    for (int k = 0; k < N; k++) {
-      const cpx<T> a = ldc<T>(U + eoff(L, mu, r * N + k, x));
-#pragma unroll
-      for (int c = 0; c < NMAX; c++)
-        if (c < N) cmac(w[c], a, S0[k * N + c]);
-    }
+    row_times_tile_acc<NMAX, T>(w, u, T0, NP, N);
 #pragma unroll
     for (int c = 0; c < NMAX; c++)
-      if (c < N) S1[r * N + c] = w[c];
+      if (c < N) T1[r * NP + c] = w[c];
   }
   __syncthreads();
-  // kick with the traceless anti-hermitian part
-  cpx<T> p[NMAX];
+  // kick with the traceless anti-hermitian part; new P rows -> T2 for the copy out
   if (act) {
     T trim = T(0);
-    for (int k = 0; k < N; k++) trim += S1[k * N + k].im;
+    for (int k = 0; k < N; k++) trim += T1[k * NP + k].im;
     trim = trim / T(N);
-    load_row<NMAX, T, S2>(p, Pin, L, mu, x, r);
 #pragma unroll
     for (int c = 0; c < NMAX; c++) {
       if (c < N) {
         const cpx<T> wrc = w[c];
-        const cpx<T> wcr = S1[c * N + r];
+        const cpx<T> wcr = T1[c * NP + r];
         T fr, fi;
         if (c == r) {
           fr = wrc.im - trim;
@@ -237,25 +363,33 @@ __device__ __forceinline__ void force_rows(const Lat& L, const S2* __restrict__ 
         p[c].im = fma(-eps_k, fi, p[c].im);
       }
     }
-    store_row<NMAX, T, S2>(Pout, p, L, mu, x, r);
+  }
+  __syncthreads();
+  if (act) {
+#pragma unroll
+    for (int c = 0; c < NMAX; c++)
+      if (c < N) T2[r * NP + c] = p[c];
+  }
+  __syncthreads();
+  if (cact) {
+#pragma unroll
+    for (int c = 0; c < NMAX; c++)
+      if (c < N) stc(Pout + eoff(L, mu, cr * N + c, cx), C2[cr * NP + c]);
   }
   if (MODE == 1) {
-    // drift: T <- U + (X/n) T, X = i eps_d P, T staged through S0
-    cpx<T> u[NMAX], tm[NMAX];
-    if (act) {
-      load_row<NMAX, T, S2>(u, U, L, mu, x, r);
+    // drift: Tm <- U + (X/n) Tm, X = i eps_d P, Tm staged through T0
+    cpx<T> tm[NMAX];
 #pragma unroll
-      for (int c = 0; c < NMAX; c++) {
-        tm[c] = u[c];
-        p[c] = mkc<T>(-eps_d * p[c].im, eps_d * p[c].re);
-      }
+    for (int c = 0; c < NMAX; c++) {
+      tm[c] = u[c];
+      p[c] = mkc<T>(-eps_d * p[c].im, eps_d * p[c].re);
     }
     for (int n = order; n >= 1; n--) {
       __syncthreads();
       if (act) {
 #pragma unroll
         for (int c = 0; c < NMAX; c++)
-          if (c < N) S0[r * N + c] = tm[c];
+          if (c < N) T0[r * NP + c] = tm[c];
       }
       __syncthreads();
       if (act) {
@@ -263,34 +397,26 @@ __device__ __forceinline__ void force_rows(const Lat& L, const S2* __restrict__ 
         cpx<T> s[NMAX];
 #pragma unroll
         for (int c = 0; c < NMAX; c++) s[c] = czero<T>();
-#pragma unroll KU
-        for (int k = 0; k < NMAX; k++) {
-          if (k >= N) break;
-          const cpx<T> xk = p[k];
-#pragma unroll
-          for (int c = 0; c < NMAX; c++)
-            if (c < N) cmac(s[c], xk, S0[k * N + c]);
-        }
+        row_times_tile_acc<NMAX, T>(s, p, T0, NP, N);
 #pragma unroll
         for (int c = 0; c < NMAX; c++) tm[c] = mkc<T>(fma(s[c].re, inv, u[c].re), fma(s[c].im, inv, u[c].im));
       }
     }
-    if (reunit) {
-      __syncthreads();
-      if (act) {
+    __syncthreads();
+    if (act) {
 #pragma unroll
-        for (int c = 0; c < NMAX; c++)
-          if (c < N) S0[r * N + c] = tm[c];
-      }
-      __syncthreads();
-      reunitarise_tile<T>(S0, S1, N, r, act, &piv_s[in_group ? g : 0], &det_s[in_group ? g : 0]);
-      if (act) {
-#pragma unroll
-        for (int c = 0; c < NMAX; c++)
-          if (c < N) tm[c] = S0[r * N + c];
-      }
+      for (int c = 0; c < NMAX; c++)
+        if (c < N) T0[r * N + c] = tm[c];
     }
-    if (act) store_row<NMAX, T, S2>(Uout, tm, L, mu, x, r);
+    __syncthreads();
+    if (reunit) reunitarise_tile<T>(T0, T0 + N * N, N, r, act, &piv_s[act ? g : 0], &det_s[act ? g : 0]);
+    // copy out (reunitarise_tile ends with a barrier)
+    if (!reunit) __syncthreads();
+    if (cact) {
+#pragma unroll
+      for (int c = 0; c < NMAX; c++)
+        if (c < N) stc(Uout + eoff(L, mu, cr * N + c, cx), C0[cr * N + c]);
+    }
   }
 }
 
@@ -300,8 +426,12 @@ __global__ void k_force(Lat L, const S2* __restrict__ U, const S2* Pin, S2* Pout
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int piv_s[64];
   __shared__ cpx<T> det_s[64];
-  force_rows<NMAX, T, S2, MODE>(L, U, Pin, Pout, Uout, eps_k, eps_d, order, reunit,
-                                (long)blockIdx.x * (blockDim.x / L.N), smem_raw, piv_s, det_s);
+  // CTAs run site-block-major: consecutive CTAs take the directions of the same sites
+  const int GS = blockDim.x / L.N;
+  const int mu = blockIdx.x % L.D;
+  const int site0 = (blockIdx.x / L.D) * GS;
+  force_rows<NMAX, T, S2, MODE>(L, U, Pin, Pout, Uout, eps_k, eps_d, order, reunit, mu, site0, smem_raw, piv_s,
+                                det_s);
 }
 
 // In-place drift U <- exp(i eps P) U, optional reunitarisation.
@@ -320,7 +450,7 @@ __global__ void k_drift(Lat L, S2* __restrict__ U, const S2* __restrict__ P, T e
   const bool act = in_group && link < (long)L.V * L.D;
   const int mu = act ? (int)(link / L.V) : 0;
   const int x = act ? (int)(link - (long)mu * L.V) : 0;
-  cpx<T>* S0 = reinterpret_cast<cpx<T>*>(smem_raw) + (size_t)(in_group ? g : 0) * 2 * N * N;
+  cpx<T>* S0 = group_tile<T>(smem_raw, in_group ? g : 0, N);
   cpx<T>* S1 = S0 + N * N;
   cpx<T> u[NMAX], tm[NMAX], p[NMAX];
   if (act) {
@@ -347,7 +477,7 @@ __global__ void k_drift(Lat L, S2* __restrict__ U, const S2* __restrict__ P, T e
       for (int c = 0; c < NMAX; c++) s[c] = czero<T>();
 #pragma unroll KU
       for (int k = 0; k < NMAX; k++) {
-        if (k >= N) break;
+        if (k >= N) continue;
         const cpx<T> xk = p[k];
 #pragma unroll
         for (int c = 0; c < NMAX; c++)
@@ -390,7 +520,7 @@ __global__ void k_reunit(Lat L, S2* __restrict__ U) {
   const bool act = in_group && link < (long)L.V * L.D;
   const int mu = act ? (int)(link / L.V) : 0;
   const int x = act ? (int)(link - (long)mu * L.V) : 0;
-  cpx<T>* S0 = reinterpret_cast<cpx<T>*>(smem_raw) + (size_t)(in_group ? g : 0) * 2 * N * N;
+  cpx<T>* S0 = group_tile<T>(smem_raw, in_group ? g : 0, N);
   cpx<T>* S1 = S0 + N * N;
   if (act)
     for (int c = 0; c < N; c++) S0[r * N + c] = ldc<T>(U + eoff(L, mu, r * N + c, x));
