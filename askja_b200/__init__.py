@@ -44,7 +44,7 @@ EXPORTS = [
     "askja_conf_read", "askja_host_alloc", "askja_host_free", "askja_plaqexp_static", "askja_peak_flops",
     "askja_batch_create", "askja_batch_destroy", "askja_batch_last_error", "askja_batch_stream",
     "askja_batch_hot_start", "askja_batch_set_links", "askja_batch_get_links", "askja_batch_run",
-    "askja_batch_plaquette",
+    "askja_batch_plaquette", "askja_autotune", "askja_set_tuning",
 ]
 
 
@@ -503,3 +503,33 @@ class Batch:
         out = (ctypes.c_double * len(self.chains))()
         self._ck(self.lib.askja_batch_plaquette(self._b, out))
         return list(out)
+
+
+class Tuning(ctypes.Structure):
+    _fields_ = [("path", ctypes.c_int), ("groups", ctypes.c_int), ("occupancy", ctypes.c_int),
+                ("ncand", ctypes.c_int), ("best_us", ctypes.c_double), ("cand_path", ctypes.c_int * 24),
+                ("cand_groups", ctypes.c_int * 24), ("cand_occ", ctypes.c_int * 24), ("cand_us", ctypes.c_double * 24)]
+
+    def as_dict(self):
+        n = self.ncand
+        return {"path": self.path, "groups": self.groups, "occupancy": self.occupancy, "best_us": self.best_us,
+                "candidates": [{"path": self.cand_path[i], "groups": self.cand_groups[i],
+                                "occupancy": self.cand_occ[i], "us": self.cand_us[i]} for i in range(n)]}
+
+
+def autotune(engine: "Engine", reps: int = 5) -> dict:
+    """askja_autotune: time the kernel mappings for this engine's (NC, DIM,
+    precision) and switch to the fastest (remembered for later engines)."""
+    L = engine.lib
+    L.askja_autotune.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(Tuning)]
+    t = Tuning()
+    engine._ck(L.askja_autotune(engine._ctx, int(reps), ctypes.byref(t)))
+    return t.as_dict()
+
+
+def set_tuning(engine: "Engine", d: dict):
+    L = engine.lib
+    L.askja_set_tuning.argtypes = [ctypes.c_void_p, ctypes.POINTER(Tuning)]
+    t = Tuning()
+    t.path, t.groups, t.occupancy = int(d["path"]), int(d.get("groups", 0)), int(d.get("occupancy", 0))
+    engine._ck(L.askja_set_tuning(engine._ctx, ctypes.byref(t)))

@@ -15,7 +15,10 @@
 #include <string.h>
 
 #include <cmath>
+#include <map>
+#include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "../../include/askja_gpu.h"
@@ -30,6 +33,10 @@ using askja::misc::TrajState;
 static_assert(sizeof(askja_traj_result) == sizeof(TrajState), "traj result layout");
 
 static thread_local std::string g_last_error;
+
+// autotuning results of this process, per (NC, DIM, precision)
+static std::mutex g_tune_mutex;
+static std::map<std::tuple<int, int, int>, askja_tuning> g_tune_cache;
 
 struct askja_ctx {
   askja_params p{};
@@ -300,6 +307,17 @@ int askja_create(const askja_params* p, askja_ctx** out) {
   c->lc.order = askja::taylor_order(p->level);
   c->lc.reunit = p->reunitarise < 0 ? (p->precision == ASKJA_FP32) : (p->reunitarise != 0);
   c->lc.force_rows = p->kernel_path == 1;
+  c->lc.rows_groups = 0;
+  c->lc.small_occ = 0;
+  if (p->kernel_path == 0) {
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    auto it = g_tune_cache.find(std::make_tuple(p->nc, p->dim, p->precision));
+    if (it != g_tune_cache.end()) {
+      c->lc.force_rows = it->second.path;
+      c->lc.rows_groups = it->second.groups;
+      c->lc.small_occ = it->second.occupancy;
+    }
+  }
   // cold start by default
   if (c->ks->identity(c->lc, c->U[0]) != cudaSuccess) return fail(set_err(c, ASKJA_ERR_CUDA, "identity launch"));
   CKC(cudaMemcpyAsync(c->Uconf, c->U[0], c->field_bytes, cudaMemcpyDeviceToDevice, c->stream));
@@ -620,6 +638,92 @@ int askja_run_trajectories(askja_ctx* c, int ntraj, int nsteps, int use_graph, a
       memcpy(log + 4 * (size_t)t, ring.data() + 4 * k, 4 * sizeof(double));
     }
   }
+  return ASKJA_OK;
+}
+
+int askja_set_tuning(askja_ctx* c, const askja_tuning* t) {
+  if (int rc = check_ctx(c)) return rc;
+  if (!t || (t->path != 0 && t->path != 1) || (t->path == 0 && c->N > 4) || t->groups < 0)
+    return set_err(c, ASKJA_ERR_ARG, "invalid tuning");
+  c->lc.force_rows = t->path;
+  c->lc.rows_groups = t->groups;
+  c->lc.small_occ = t->occupancy ? 1 : 0;
+  drop_graphs(c);
+  return ASKJA_OK;
+}
+
+int askja_autotune(askja_ctx* c, int reps, askja_tuning* out) {
+  if (int rc = check_ctx(c)) return rc;
+  if (reps < 1) reps = 5;
+  DevGuard g(c->p.device);
+  struct Cand {
+    int path, groups, occ;
+  };
+  std::vector<Cand> cands;
+  const bool fp64 = c->p.precision == ASKJA_FP64;
+  if (c->N <= 4) {
+    cands.push_back({0, 0, 0});
+    cands.push_back({0, 0, 1});
+  }
+  std::vector<int> seen;
+  for (int want : {0, 2, 4, 8, 16, 32, 64}) {
+    const int eff = askja::rows_effective_groups(c->N, fp64, want);
+    bool dup = false;
+    for (int s : seen) dup |= s == eff;
+    if (dup) continue;
+    seen.push_back(eff);
+    cands.push_back({1, eff, 0});
+  }
+  if (cands.size() > 24) cands.resize(24);
+  // scratch: Pi holds a copy of pi, the partner link buffer receives the output
+  CK(cudaMemcpyAsync(c->P2, c->P, c->field_bytes, cudaMemcpyDeviceToDevice, c->stream));
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  const askja::LaunchCtx saved = c->lc;
+  askja_tuning res{};
+  res.best_us = 1e300;
+  int best = 0;
+  for (size_t i = 0; i < cands.size(); i++) {
+    askja::LaunchCtx lc = saved;
+    lc.force_rows = cands[i].path;
+    lc.rows_groups = cands[i].groups;
+    lc.small_occ = cands[i].occ;
+    cudaError_t e = c->ks->force(lc, 1, cur_u(c), c->P2, c->P2, c->U[1 - c->cur], 0.5 * c->p.dt, c->p.dt);
+    if (e == cudaSuccess) e = cudaEventRecord(e0, c->stream);
+    for (int r = 0; r < reps && e == cudaSuccess; r++)
+      e = c->ks->force(lc, 1, cur_u(c), c->P2, c->P2, c->U[1 - c->cur], 0.5 * c->p.dt, c->p.dt);
+    if (e == cudaSuccess) e = cudaEventRecord(e1, c->stream);
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    if (e != cudaSuccess) {
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      return set_err(c, ASKJA_ERR_CUDA, "autotune candidate %zu: %s", i, cudaGetErrorString(e));
+    }
+    const double us = 1e3 * ms / reps;
+    res.cand_path[i] = cands[i].path;
+    res.cand_groups[i] = cands[i].groups;
+    res.cand_occ[i] = cands[i].occ;
+    res.cand_us[i] = us;
+    if (us < res.best_us) {
+      res.best_us = us;
+      best = (int)i;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  res.ncand = (int)cands.size();
+  res.path = cands[best].path;
+  res.groups = cands[best].groups;
+  res.occupancy = cands[best].occ;
+  if (int rc = askja_set_tuning(c, &res)) return rc;
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    g_tune_cache[std::make_tuple(c->N, c->D, c->p.precision)] = res;
+  }
+  if (out) *out = res;
   return ASKJA_OK;
 }
 

@@ -22,9 +22,11 @@ inline unsigned blocks_for(long n, int threads) { return (unsigned)((n + threads
 template <typename T>
 struct Rows {
   // groups per block and dynamic shared memory for the row-per-thread kernels
-  static void shape(int N, int* G, size_t* smem) {
+  static void shape(int N, int* G, size_t* smem, int want = 0) {
     const size_t per = rows::smem_per_group<T>(N);
-    int g = std::max(1, 128 / N);
+    int g = want > 0 ? want : std::max(1, 128 / N);
+    // at most 256 threads: launchable at any register count up to 255
+    g = std::min(g, std::max(1, 256 / N));
     g = std::min(g, 64);
     while (g > 1 && (size_t)g * per > ROWS_SMEM_BUDGET) g--;
     *G = g;
@@ -46,7 +48,7 @@ cudaError_t rows_force(const LaunchCtx& c, int mode, const void* U, const void* 
   using S2 = typename Storage<T>::type;
   int G;
   size_t smem;
-  Rows<T>::shape(c.lat.N, &G, &smem);
+  Rows<T>::shape(c.lat.N, &G, &smem, c.rows_groups);
   // G consecutive sites of one direction per CTA, all directions of a site block adjacent
   const unsigned grid = blocks_for(c.lat.V, G) * c.lat.D;
   cudaError_t e;
@@ -69,7 +71,7 @@ cudaError_t rows_drift(const LaunchCtx& c, void* U, const void* P, double eps) {
   using S2 = typename Storage<T>::type;
   int G;
   size_t smem;
-  Rows<T>::shape(c.lat.N, &G, &smem);
+  Rows<T>::shape(c.lat.N, &G, &smem, c.rows_groups);
   auto k = rows::k_drift<NMAX, T, S2>;
   cudaError_t e;
   if ((e = set_smem(k, smem)) != cudaSuccess) return e;
@@ -85,12 +87,22 @@ cudaError_t small_force(const LaunchCtx& c, int mode, const void* U, const void*
   // site tiles: 32 sites per CTA, one warp per direction (warps loop when DIM > 4)
   const unsigned grid = blocks_for(c.lat.V, 32);
   const int threads = 32 * std::min(c.lat.D, 4);
-  if (mode == 0)
-    small::k_force<N, T, S2, 0><<<grid, threads, 0, c.stream>>>(c.lat, (const S2*)U, (const S2*)Pin, (S2*)Pout,
-                                                                      (S2*)Uout, (T)ek, (T)ed, c.order, c.reunit);
-  else
-    small::k_force<N, T, S2, 1><<<grid, threads, 0, c.stream>>>(c.lat, (const S2*)U, (const S2*)Pin, (S2*)Pout,
-                                                                      (S2*)Uout, (T)ek, (T)ed, c.order, c.reunit);
+  const S2* u = (const S2*)U;
+  const S2* pi = (const S2*)Pin;
+  if (c.small_occ) {
+    if (mode == 0)
+      small::k_force_occ<N, T, S2, 0><<<grid, threads, 0, c.stream>>>(c.lat, u, pi, (S2*)Pout, (S2*)Uout, (T)ek,
+                                                                        (T)ed, c.order, c.reunit);
+    else
+      small::k_force_occ<N, T, S2, 1><<<grid, threads, 0, c.stream>>>(c.lat, u, pi, (S2*)Pout, (S2*)Uout, (T)ek,
+                                                                        (T)ed, c.order, c.reunit);
+  } else if (mode == 0) {
+    small::k_force<N, T, S2, 0><<<grid, threads, 0, c.stream>>>(c.lat, u, pi, (S2*)Pout, (S2*)Uout, (T)ek, (T)ed,
+                                                                c.order, c.reunit);
+  } else {
+    small::k_force<N, T, S2, 1><<<grid, threads, 0, c.stream>>>(c.lat, u, pi, (S2*)Pout, (S2*)Uout, (T)ek, (T)ed,
+                                                                c.order, c.reunit);
+  }
   return cudaGetLastError();
 }
 

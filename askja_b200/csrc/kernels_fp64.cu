@@ -15,4 +15,14 @@ size_t partial_doubles(const Lat& L) {
   return std::max(plaq, std::max(links, gauss)) + 64;
 }
 
+int rows_effective_groups(int N, bool fp64, int want) {
+  int G;
+  size_t smem;
+  if (fp64)
+    detail::Rows<double>::shape(N, &G, &smem, want);
+  else
+    detail::Rows<float>::shape(N, &G, &smem, want);
+  return G;
+}
+
 }  // namespace askja

@@ -13,9 +13,11 @@ namespace askja {
 struct LaunchCtx {
   Lat lat;
   cudaStream_t stream;
-  int order;       // effective Taylor order
-  int reunit;      // reunitarise after each link update
-  int force_rows;  // use the row-per-thread kernels even for NC <= 4
+  int order;        // effective Taylor order
+  int reunit;       // reunitarise after each link update
+  int force_rows;   // use the row-per-thread kernels even for NC <= 4
+  int rows_groups;  // row kernels: sites per CTA (0: default 128/NC)
+  int small_occ;    // thread-per-link kernels: 1 = higher-occupancy register budget
 };
 
 // Scalar reductions return their values in device memory:
@@ -44,6 +46,10 @@ struct KernelSet {
 
 // size (in doubles) of the partial buffer the reductions need
 size_t partial_doubles(const Lat& L);
+
+// sites per CTA the row-per-thread kernels actually use for a requested value
+// (0: default), after the thread-count and shared-memory limits
+int rows_effective_groups(int N, bool fp64, int want);
 
 extern const KernelSet kernels_fp64;
 extern const KernelSet kernels_fp32;

@@ -296,6 +296,18 @@ __global__ void __launch_bounds__(128) k_force(Lat L, const S2* __restrict__ U, 
       L, U, Pin, Pout, Uout, eps_k, eps_d, order, reunit, mu, x);
 }
 
+// The same kernel with a tighter register budget for more resident CTAs
+// (6 per SM in FP32, 3 in FP64); the autotuner picks it where it is faster.
+template <int N, typename T, typename S2, int MODE>
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 6 : 3)
+    k_force_occ(Lat L, const S2* __restrict__ U, const S2* Pin, S2* Pout, S2* __restrict__ Uout, T eps_k, T eps_d,
+                int order, int reunit) {
+  const int x = blockIdx.x * 32 + (threadIdx.x & 31);
+  if (x >= L.V) return;
+  for (int mu = threadIdx.x >> 5; mu < L.D; mu += (blockDim.x >> 5))
+    force_link<N, T, S2, MODE>(L, U, Pin, Pout, Uout, eps_k, eps_d, order, reunit, mu, x);
+}
+
 // In-place drift: U <- exp(i eps P) U (updateUandcopyDown; the copy pi = Pi is
 // done by the caller).  Optionally reunitarises.
 template <int N, typename T, typename S2>

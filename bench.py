@@ -218,13 +218,16 @@ def run_ours(args):
         with ab.Engine(nc, dims, beta=cfg["beta"], dt=cfg["dt"], level=cfg["level"], precision=prec, device=dev,
                        seed=seed) as e:
             e.hot_start(seed + 1)
+            e.initializeE(seed, 0)
+            tuning = ab.autotune(e, reps=3)  # untimed: picks the kernel mapping for this (NC, DIM, precision)
             K = args.steps if prec == "fp32" else max(3, args.steps // 2)
             clocks = Clocks(dev) if prec == "fp32" else None
             ms, last, log = time_trajectories(e, e.stream_ptr, dev, nsteps, K, args.warmup, world, clocks)
             ms_max = max_over_ranks(ms, world)
             lu = aggregate_rate(links * nsteps * K, world, ms_max / 1e3)
             r = dict(ms=ms_max, K=K, lu=lu, acc=last["n_acc"] / max(1, last["n_tot"]),
-                     dh_mean=float(np.mean(log[:, 2])), dh_abs=float(np.mean(np.abs(log[:, 2]))))
+                     dh_mean=float(np.mean(log[:, 2])), dh_abs=float(np.mean(np.abs(log[:, 2]))),
+                     tuning={k: tuning[k] for k in ("path", "groups", "occupancy", "best_us")})
             if clocks is not None:
                 r["clocks"] = clocks.summary()
                 # dominant kernel: fused kick+drift, timed alone
@@ -264,6 +267,7 @@ def run_ours(args):
         "fp64": {"value": f64["lu"], "ms_per_step": f64["ms"] / f64["K"], "steps": f64["K"],
                  "acceptance": f64["acc"], "mean_abs_dH": f64["dh_abs"]},
         "mixed_over_fp64": f32["lu"] / f64["lu"],
+        "tuning": {"fp32": f32["tuning"], "fp64": f64["tuning"]},
         "acceptance": f32["acc"],
         "mean_abs_dH": f32["dh_abs"],
         "plaquette": f32["plaq"],

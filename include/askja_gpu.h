@@ -152,6 +152,29 @@ ASKJA_API int askja_leapfrog(askja_ctx* ctx, int nsteps, double eps);
  * reference's globals would. */
 ASKJA_API int askja_md_steps(askja_ctx* ctx, int nsteps, double eps);
 
+/* ---- autotuning (not in the reference) ---------------------------------- */
+/* Kernel mapping for the force / link-update kernel of one (NC, DIM,
+ * precision): thread-per-link (NC <= 4, all matrices in registers) or
+ * row-per-thread (NC threads per link, shared-memory tiles), the number of
+ * sites per CTA of the latter, and the register budget of the former. */
+typedef struct {
+  int path;       /* 0 thread-per-link, 1 row-per-thread */
+  int groups;     /* row-per-thread: sites per CTA (0 = default) */
+  int occupancy;  /* thread-per-link: 0 default registers, 1 tighter budget / more CTAs */
+  int ncand;      /* candidates timed */
+  double best_us; /* fused kick+drift launch time of the choice, microseconds */
+  int cand_path[24], cand_groups[24], cand_occ[24];
+  double cand_us[24];
+} askja_tuning;
+
+/* Times every candidate on this context's lattice (reps launches each, on
+ * scratch copies of the fields -- u and pi are left unchanged, Pi is
+ * overwritten), switches the context to the fastest and remembers it for
+ * later contexts with the same (NC, DIM, precision) in this process. */
+ASKJA_API int askja_autotune(askja_ctx* ctx, int reps, askja_tuning* out);
+/* Applies a previously found mapping (for example read back from a file). */
+ASKJA_API int askja_set_tuning(askja_ctx* ctx, const askja_tuning* t);
+
 /* ---- batched independent chains (not in the reference) ----------------- */
 /* Many independent HMC chains of uneven shape -- a beta scan, several colour
  * numbers, dimensions and volumes -- advanced together: per MD step one force

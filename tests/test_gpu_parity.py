@@ -169,3 +169,32 @@ def test_trajectory_matches_oracle():
         assert r["n_tot"] == 1 and r["traj"] == 1
         assert rel(e.get_saved_links(), uu if acc else u) < 1e-12
         assert rel(e.get_links(), uu if acc else u) < 1e-12
+
+
+@pytest.mark.parametrize("nc,dims,precision", [(24, [2, 2, 2], "fp64"), (32, [2, 2, 2], "fp64"), (64, [2, 2], "fp64"),
+                                               (32, [2, 2, 2], "fp32"), (64, [2, 2], "fp32")])
+def test_large_nc_vs_oracle(nc, dims, precision):
+    """Large colour numbers (config 5's SU(32)/SU(64)) on tiny lattices."""
+    rng = np.random.default_rng(nc)
+    O = Oracle(nc, dims)
+    nl = O.vol * O.dim
+    u = fields.haar(nc, nl, rng).reshape(O.shape)
+    beta = 2.0 * nc * nc
+    pi = fields.momenta(nc, nl, beta, rng, O)
+    tol = TOL64 if precision == "fp64" else 5e-5
+    with ab.Engine(nc, dims, beta=beta, dt=0.005, level=8, precision=precision, reunitarise=False) as e:
+        e.set_links(u)
+        e.set_momenta(pi, 0)
+        e.updateE(0.005)
+        Pi = O.updateE(u, pi, 0.005)
+        assert rel(e.get_momenta(1), Pi) < tol
+        e.updateUandcopyDown(0.005)
+        assert rel(e.get_links(), O.updateU(u, Pi, 0.005, 8)) < (TOL64 if precision == "fp64" else 5e-6)
+        e.set_links(u)
+        e.set_momenta(pi, 0)
+        e.leapfrog(2, 0.005)
+        uu, pp = u, O.updateE(u, pi, 0.0025)
+        for k in range(2):
+            uu = O.updateU(uu, pp, 0.005, 8)
+            pp = O.updateE(uu, pp, 0.005 if k < 1 else 0.0025)
+        assert rel(e.get_links(), uu) < (TOL64 if precision == "fp64" else 5e-6)
