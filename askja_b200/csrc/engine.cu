@@ -60,6 +60,7 @@ struct askja_ctx {
   int logcap = 0;
   void* staging = nullptr;  // U-conf layout staging buffer (V*D*NC*NC double2)
   unsigned long long* nonfinite = nullptr;
+  unsigned* tc_status = nullptr;  // tensor-core kernels: set when a bounded wait gave up
   cudaStream_t stream = nullptr;
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
   int g_nsteps[2] = {-1, -1};
@@ -166,11 +167,25 @@ void drop_graphs(askja_ctx* c) {
   }
 }
 
-int read_state(askja_ctx* c, askja_traj_result* out) {
-  if (!out) return ASKJA_OK;
-  CK(cudaMemcpyAsync(out, c->st, sizeof(TrajState), cudaMemcpyDeviceToHost, c->stream));
+// synchronise the stream and report a tensor-core kernel that stopped after a
+// bounded wait (its outputs are incomplete)
+int sync_checked(askja_ctx* c) {
   CK(cudaStreamSynchronize(c->stream));
+  if (c->lc.force_rows == 2) {
+    unsigned st = 0;
+    CK(cudaMemcpy(&st, c->tc_status, sizeof st, cudaMemcpyDeviceToHost));
+    if (st) {
+      CK(cudaMemset(c->tc_status, 0, sizeof st));
+      return set_err(c, ASKJA_ERR_CUDA, "tensor-core link update gave up waiting for its MMA");
+    }
+  }
   return ASKJA_OK;
+}
+
+int read_state(askja_ctx* c, askja_traj_result* out) {
+  if (!out) return sync_checked(c);
+  CK(cudaMemcpyAsync(out, c->st, sizeof(TrajState), cudaMemcpyDeviceToHost, c->stream));
+  return sync_checked(c);
 }
 
 int upload_conf(askja_ctx* c, const double* conf, void* dst) {
@@ -214,8 +229,7 @@ void* askja_stream(askja_ctx* c) { return c ? (void*)c->stream : nullptr; }
 int askja_sync(askja_ctx* c) {
   if (int rc = check_ctx(c)) return rc;
   DevGuard g(c->p.device);
-  CK(cudaStreamSynchronize(c->stream));
-  return ASKJA_OK;
+  return sync_checked(c);
 }
 
 void askja_destroy(askja_ctx* c) {
@@ -224,7 +238,7 @@ void askja_destroy(askja_ctx* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   drop_graphs(c);
   void* bufs[] = {c->U[0], c->U[1], c->P, c->P2, c->Uconf, c->nbr, c->partial, c->sums, c->lines,
-                  c->st,   c->logbuf, c->staging, c->nonfinite};
+                  c->st,   c->logbuf, c->staging, c->nonfinite, c->tc_status};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -247,6 +261,10 @@ int askja_create(const askja_params* p, askja_ctx** out) {
   if (!(p->beta > 0.0) || !std::isfinite(p->beta)) return set_err(nullptr, ASKJA_ERR_ARG, "BETA must be > 0");
   if (p->precision != ASKJA_FP64 && p->precision != ASKJA_FP32)
     return set_err(nullptr, ASKJA_ERR_ARG, "unknown precision %d", p->precision);
+  if (p->kernel_path < 0 || p->kernel_path > 2)
+    return set_err(nullptr, ASKJA_ERR_ARG, "unknown kernel path %d", p->kernel_path);
+  if (p->kernel_path == 2 && !askja::tc_supported(p->nc, p->dim, p->precision == ASKJA_FP64))
+    return set_err(nullptr, ASKJA_ERR_ARG, "tensor-core path needs FP32, NC = 32 or 64 and DIM >= 2");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
     return set_err(nullptr, ASKJA_ERR_NODEVICE, "no CUDA device available (the engine has no CPU fallback)");
@@ -306,7 +324,14 @@ int askja_create(const askja_params* p, askja_ctx** out) {
   c->lc.stream = c->stream;
   c->lc.order = askja::taylor_order(p->level);
   c->lc.reunit = p->reunitarise < 0 ? (p->precision == ASKJA_FP32) : (p->reunitarise != 0);
-  c->lc.force_rows = p->kernel_path == 1;
+  CKC(cudaMalloc(&c->tc_status, sizeof(unsigned)));
+  CKC(cudaMemset(c->tc_status, 0, sizeof(unsigned)));
+  c->lc.scratch = c->staging;
+  c->lc.status = c->tc_status;
+  // untuned default: tensor cores where they exist, else thread-per-link for NC <= 4
+  c->lc.force_rows = p->kernel_path != 0 ? p->kernel_path
+                     : askja::tc_supported(p->nc, p->dim, p->precision == ASKJA_FP64) ? 2
+                                                                                       : 0;
   c->lc.rows_groups = 0;
   c->lc.small_occ = 0;
   if (p->kernel_path == 0) {
@@ -643,7 +668,8 @@ int askja_run_trajectories(askja_ctx* c, int ntraj, int nsteps, int use_graph, a
 
 int askja_set_tuning(askja_ctx* c, const askja_tuning* t) {
   if (int rc = check_ctx(c)) return rc;
-  if (!t || (t->path != 0 && t->path != 1) || (t->path == 0 && c->N > 4) || t->groups < 0)
+  if (!t || t->path < 0 || t->path > 2 || (t->path == 0 && c->N > 4) || t->groups < 0 ||
+      (t->path == 2 && !askja::tc_supported(c->N, c->D, c->p.precision == ASKJA_FP64)))
     return set_err(c, ASKJA_ERR_ARG, "invalid tuning");
   c->lc.force_rows = t->path;
   c->lc.rows_groups = t->groups;
@@ -665,6 +691,7 @@ int askja_autotune(askja_ctx* c, int reps, askja_tuning* out) {
     cands.push_back({0, 0, 0});
     cands.push_back({0, 0, 1});
   }
+  if (askja::tc_supported(c->N, c->D, fp64)) cands.push_back({2, 0, 0});
   std::vector<int> seen;
   for (int want : {0, 2, 4, 8, 16, 32, 64}) {
     const int eff = askja::rows_effective_groups(c->N, fp64, want);

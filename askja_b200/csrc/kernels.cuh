@@ -8,6 +8,7 @@
 #include "misc.cuh"
 #include "rows.cuh"
 #include "small.cuh"
+#include "tc.cuh"
 
 namespace askja {
 
@@ -114,10 +115,51 @@ cudaError_t small_drift(const LaunchCtx& c, void* U, const void* P, double eps) 
   return cudaGetLastError();
 }
 
+// Tensor-core link update (FP32 storage): per-link copy of U into the
+// scratch buffer, then one persistent launch over all links.
+// mode 0 kick, 1 kick + drift, 2 drift only (Uout may be U).
+template <int NC>
+cudaError_t tc_link(const LaunchCtx& c, int mode, const void* U, const void* Pin, void* Pout, void* Uout, double ek,
+                    double ed) {
+  const Lat& L = c.lat;
+  if (!c.scratch || !c.status) return cudaErrorInvalidValue;
+  float2* aos = static_cast<float2*>(c.scratch);
+  int dev = 0, nsm = 0;
+  cudaError_t e;
+  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+  if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+  const int chunks = (NC * NC + 31) / 32;
+  const int z = std::max(1, std::min(chunks, (4 * nsm + L.B * L.D - 1) / (L.B * L.D)));
+  tc::k_to_aos<<<dim3(L.B, L.D, z), 256, 0, c.stream>>>(L, static_cast<const float2*>(U), aos);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  auto k = mode == 0 ? tc::k_link<NC, 0> : mode == 1 ? tc::k_link<NC, 1> : tc::k_link<NC, 2>;
+  const size_t smem = tc::Shape<NC>::SMEM;
+  if ((e = set_smem(k, smem)) != cudaSuccess) return e;
+  int per = 0;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, tc::THREADS, smem)) != cudaSuccess) return e;
+  const long grid = std::min(nlinks(L), (long)nsm * std::max(per, 1));
+  k<<<(unsigned)grid, tc::THREADS, smem, c.stream>>>(L, aos, static_cast<const float2*>(Pin),
+                                                      static_cast<float2*>(Pout), static_cast<float2*>(Uout),
+                                                      (float)ek, (float)ed, c.order, c.reunit, c.status);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t tc_dispatch(const LaunchCtx& c, int mode, const void* U, const void* Pin, void* Pout, void* Uout,
+                        double ek, double ed) {
+  if constexpr (sizeof(T) == 4) {
+    if (c.lat.N == 32) return tc_link<32>(c, mode, U, Pin, Pout, Uout, ek, ed);
+    if (c.lat.N == 64) return tc_link<64>(c, mode, U, Pin, Pout, Uout, ek, ed);
+  }
+  return cudaErrorInvalidValue;
+}
+
 template <typename T>
 cudaError_t force(const LaunchCtx& c, int mode, const void* U, const void* Pin, void* Pout, void* Uout, double ek,
                   double ed) {
   const int N = c.lat.N;
+  if (c.force_rows == 2 && tc_supported(N, c.lat.D, sizeof(T) == 8))
+    return tc_dispatch<T>(c, mode, U, Pin, Pout, Uout, ek, ed);
   if (!c.force_rows) {
     if (N == 2) return small_force<2, T>(c, mode, U, Pin, Pout, Uout, ek, ed);
     if (N == 3) return small_force<3, T>(c, mode, U, Pin, Pout, Uout, ek, ed);
@@ -133,6 +175,8 @@ cudaError_t force(const LaunchCtx& c, int mode, const void* U, const void* Pin, 
 template <typename T>
 cudaError_t drift(const LaunchCtx& c, void* U, const void* P, double eps) {
   const int N = c.lat.N;
+  if (c.force_rows == 2 && tc_supported(N, c.lat.D, sizeof(T) == 8))
+    return tc_dispatch<T>(c, 2, U, P, nullptr, U, 0.0, eps);
   if (!c.force_rows) {
     if (N == 2) return small_drift<2, T>(c, U, P, eps);
     if (N == 3) return small_drift<3, T>(c, U, P, eps);

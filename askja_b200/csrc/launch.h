@@ -15,10 +15,16 @@ struct LaunchCtx {
   cudaStream_t stream;
   int order;        // effective Taylor order
   int reunit;       // reunitarise after each link update
-  int force_rows;   // use the row-per-thread kernels even for NC <= 4
+  int force_rows;   // kernel mapping: 0 thread-per-link (NC <= 4), 1 row-per-thread,
+                    // 2 tensor cores (FP32, NC = 32 or 64, DIM >= 2)
   int rows_groups;  // row kernels: sites per CTA (0: default 128/NC)
   int small_occ;    // thread-per-link kernels: 1 = higher-occupancy register budget
+  void* scratch;    // tensor-core path: per-link contiguous copy of U (V*D*NC*NC float2)
+  unsigned* status; // tensor-core path: nonzero after a bounded wait gave up
 };
+
+// whether the tensor-core mapping exists for this shape and precision
+inline bool tc_supported(int N, int D, bool fp64) { return !fp64 && (N == 32 || N == 64) && D >= 2; }
 
 // Scalar reductions return their values in device memory:
 //   plaq     -> out[0] temporal, out[1] spatial

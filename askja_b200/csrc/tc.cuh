@@ -1,0 +1,699 @@
+// Tensor-core (tcgen05) link update for large colour number, FP32 storage,
+// NC = 32 and 64.  Same physics as rows::force_rows (sun.cpp:672-790,
+// sunmat.h:200-248, 355-371): the staple sum, the traceless anti-hermitian
+// force, the momentum kick, the order-LEVEL Taylor exponential and the link
+// update, with every NC x NC complex product on the 5th-generation tensor
+// cores.
+//
+// Complex product C = X Y as one real MMA of shape M = 2NC, N = NC, K = NC,
+// issued twice (once per part of Y):
+//     [Cr; Ci] = [Xr; Xi] Yr + [-Xi; Xr] Yi
+// so the left operand lives in shared memory as the triple block
+// (-Xi; Xr; Xi) (3NC rows): rows NC..3NC-1 are [Xr; Xi] and rows 0..2NC-1
+// are [-Xi; Xr].  The accumulator [Cr; Ci] sits in tensor memory: row r of
+// the 2NC rows in TMEM lane r (M = 128) or lane 32(r/16) + r%16 (M = 64),
+// column c in TMEM column c.
+//
+// Precision: split TF32 x 3 with FP32 accumulation.  Every operand x is
+// stored as hi = tf32(x) and lo = tf32(x - hi); each product accumulates
+// lo*hi + hi*lo + hi*hi (the lo*lo term, ~2^-22 relative, is dropped).
+//
+// Shared-memory operand layout: the K-major no-swizzle canonical layout of
+// the tcgen05 matrix descriptors -- 8 rows x 16 bytes core matrices; the
+// core matrices of one 8-row group follow each other along K at LBO = 144
+// bytes (128 + 16 of padding, so that the transposed scalar stores of an
+// epilogue hit 32 different banks), 8-row groups are SBO = (NC/4)*LBO apart.
+//
+// One CTA (256 threads = 8 warps) owns one link at a time and walks the
+// links of the lattice with a grid stride.  Thread 0 issues the MMAs and
+// commits them to one mbarrier; all threads wait on it (bounded: after about
+// a second the kernel records an error in *status and stops), read the
+// accumulator with tcgen05.ld (warp w reads TMEM lanes 32(w%4).., columns
+// (w/4)*NC/2 ..), and write the next operand.  Neighbour links are read from
+// a per-link contiguous copy of U (k_to_aos), P and the outputs use the
+// blocked field layout of common.cuh.
+//
+// Reunitarisation after the link update is one Newton-Schulz polar step
+// U <- U (3 - U^dag U) / 2 on the tensor cores (unitarity back to FP32
+// rounding; the determinant phase is not re-fixed here: exp(i eps P) of a
+// traceless P has determinant 1 up to the Taylor remainder, so the phase only
+// drifts by rounding; askja_reunitarise fixes it on demand).
+#pragma once
+
+#include "common.cuh"
+
+namespace askja {
+namespace tc {
+
+constexpr int THREADS = 256;
+constexpr uint32_t LBO = 144;
+
+template <int NC>
+struct Shape {
+  static constexpr int KC = NC / 4;  // 16-byte chunks along K
+  static constexpr int KS = NC / 8;  // MMA k-steps (K = 8 TF32 each)
+  static constexpr uint32_t SBO = KC * LBO;
+  static constexpr uint32_t A_BYTES = (3 * NC / 8) * SBO;  // one split of the triple block
+  static constexpr uint32_t B_BYTES = (NC / 8) * SBO;      // one split of one part
+  static constexpr int PS = NC + 4;                         // plain tile row stride (floats)
+  static constexpr uint32_t PLAIN_BYTES = 2u * NC * PS * 4;
+  static constexpr uint32_t SMEM = 2 * A_BYTES + 4 * B_BYTES + PLAIN_BYTES + 32;
+  static constexpr int TMEM_COLS = 2 * NC;  // T at column 0, S at column NC
+  static constexpr int UPT = NC * NC / 4 / THREADS;  // 4-element units per thread
+  static constexpr int EPT = NC * NC / THREADS;      // elements per thread
+  static constexpr int HALF = NC / 2;                // accumulator columns per thread
+};
+
+// ---------------------------------------------------------------- PTX ----
+__device__ __forceinline__ uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(saddr(bar)) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.b32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(saddr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// bounded wait: false after ~2^31 clock cycles (about a second)
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  const long long t0 = clock64();
+  while (!mbar_try(bar, parity))
+    if (clock64() - t0 > (1LL << 31)) return false;
+  return true;
+}
+
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(saddr(slot)), "r"(ncols)
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+
+// shared-memory matrix descriptor: K-major, no swizzle, sm_100 version bits
+__device__ __forceinline__ uint64_t sdesc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+__device__ __forceinline__ void mma_tf32(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                         uint32_t acc) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n}" ::"r"(dtmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc), "r"(0u)
+      : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(saddr(bar))
+               : "memory");
+}
+
+// 32 lanes x 16 / 32 columns of 32-bit accumulator; the wait carries the
+// registers so that no use is scheduled before it
+__device__ __forceinline__ void tmem_ld(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr)
+      : "memory");
+  asm volatile("tcgen05.wait::ld.sync.aligned;"
+               : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]),
+                 "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]),
+                 "+r"(r[15])
+               :
+               : "memory");
+#pragma unroll
+  for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+__device__ __forceinline__ void tmem_ld(uint32_t taddr, float (&v)[32]) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,"
+      "%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr)
+      : "memory");
+  asm volatile("tcgen05.wait::ld.sync.aligned;"
+               : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]),
+                 "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]),
+                 "+r"(r[15]), "+r"(r[16]), "+r"(r[17]), "+r"(r[18]), "+r"(r[19]), "+r"(r[20]), "+r"(r[21]),
+                 "+r"(r[22]), "+r"(r[23]), "+r"(r[24]), "+r"(r[25]), "+r"(r[26]), "+r"(r[27]), "+r"(r[28]),
+                 "+r"(r[29]), "+r"(r[30]), "+r"(r[31])
+               :
+               : "memory");
+#pragma unroll
+  for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ float tf32r(float x) {
+  uint32_t h;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(x));
+  return __uint_as_float(h);
+}
+__device__ __forceinline__ void split(float x, float& hi, float& lo) {
+  hi = tf32r(x);
+  lo = tf32r(x - hi);
+}
+
+// ------------------------------------------------------------ layout ----
+// byte offset of element (row, k) of a canonical operand
+template <int NC>
+__device__ __forceinline__ uint32_t opoff(int row, int k) {
+  return (uint32_t)(row >> 3) * Shape<NC>::SBO + (uint32_t)(k >> 2) * LBO + (uint32_t)(row & 7) * 16 +
+         (uint32_t)(k & 3) * 4;
+}
+
+struct Smem {
+  unsigned char* A;  // [2 splits][A_BYTES]
+  unsigned char* B;  // [re hi, re lo, im hi, im lo][B_BYTES]
+  float* plain;      // [2 planes][NC][PS]
+  uint64_t* bar;
+  uint32_t* slot;
+};
+
+// four consecutive K elements of one row, hi and lo splits
+template <int NC>
+__device__ __forceinline__ void st4(unsigned char* base, uint32_t split_bytes, uint32_t off, float4 x) {
+  float4 h, l;
+  split(x.x, h.x, l.x);
+  split(x.y, h.y, l.y);
+  split(x.z, h.z, l.z);
+  split(x.w, h.w, l.w);
+  *reinterpret_cast<float4*>(base + off) = h;
+  *reinterpret_cast<float4*>(base + split_bytes + off) = l;
+}
+template <int NC>
+__device__ __forceinline__ void st1(unsigned char* base, uint32_t split_bytes, uint32_t off, float x) {
+  float h, l;
+  split(x, h, l);
+  *reinterpret_cast<float*>(base + off) = h;
+  *reinterpret_cast<float*>(base + split_bytes + off) = l;
+}
+
+__device__ __forceinline__ float4 neg4(float4 a) { return make_float4(-a.x, -a.y, -a.z, -a.w); }
+
+// left operand X, row m, K elements 4kc..4kc+3
+template <int NC>
+__device__ __forceinline__ void put_A(const Smem& s, int m, int kc, float4 re, float4 im) {
+  using SH = Shape<NC>;
+  st4<NC>(s.A, SH::A_BYTES, opoff<NC>(NC + m, 4 * kc), re);
+  st4<NC>(s.A, SH::A_BYTES, opoff<NC>(2 * NC + m, 4 * kc), im);
+  st4<NC>(s.A, SH::A_BYTES, opoff<NC>(m, 4 * kc), neg4(im));
+}
+// right operand Y stored K-major: Bs[j][k] = Y[k][j]
+template <int NC>
+__device__ __forceinline__ void put_B(const Smem& s, int j, int kc, float4 re, float4 im) {
+  using SH = Shape<NC>;
+  const uint32_t off = opoff<NC>(j, 4 * kc);
+  st4<NC>(s.B, SH::B_BYTES, off, re);
+  st4<NC>(s.B + 2 * SH::B_BYTES, SH::B_BYTES, off, im);
+}
+
+// ------------------------------------------------- global -> registers ----
+// A fragment of one NC x NC matrix in per-link contiguous row-major storage,
+// UPT units of four complex numbers per thread.  Row-kind units read
+// Y[r][4kc..4kc+3] (contiguous), column-kind units read Y[4kc..4kc+3][r].
+template <int NC>
+struct Frag {
+  float4 re[Shape<NC>::UPT], im[Shape<NC>::UPT];
+};
+
+template <int NC>
+__device__ __forceinline__ void unit_rc(int u, bool rowkind, int& r, int& kc) {
+  if (rowkind) {
+    r = u / Shape<NC>::KC;
+    kc = u % Shape<NC>::KC;
+  } else {
+    r = u % NC;
+    kc = u / NC;
+  }
+}
+
+template <int NC>
+__device__ __forceinline__ void fetch(Frag<NC>& f, const float2* __restrict__ y, bool rowkind) {
+#pragma unroll
+  for (int i = 0; i < Shape<NC>::UPT; i++) {
+    int r, kc;
+    unit_rc<NC>(threadIdx.x + THREADS * i, rowkind, r, kc);
+    if (rowkind) {
+      const float4* p = reinterpret_cast<const float4*>(y + r * NC + 4 * kc);
+      const float4 a = __ldg(p), b = __ldg(p + 1);
+      f.re[i] = make_float4(a.x, a.z, b.x, b.z);
+      f.im[i] = make_float4(a.y, a.w, b.y, b.w);
+    } else {
+      const float2 a = __ldg(y + (4 * kc + 0) * NC + r), b = __ldg(y + (4 * kc + 1) * NC + r);
+      const float2 c = __ldg(y + (4 * kc + 2) * NC + r), d = __ldg(y + (4 * kc + 3) * NC + r);
+      f.re[i] = make_float4(a.x, b.x, c.x, d.x);
+      f.im[i] = make_float4(a.y, b.y, c.y, d.y);
+    }
+  }
+}
+
+// operand kinds: left X = Y (row-kind) or X = Y^dag (column-kind);
+// right B = Y (column-kind) or B = Y^dag (row-kind)
+enum Kind { A_NORM = 0, A_DAG = 1, B_NORM = 2, B_DAG = 3 };
+__device__ __forceinline__ bool kind_rowwise(int kind) { return kind == A_NORM || kind == B_DAG; }
+
+template <int NC>
+__device__ __forceinline__ void put(const Smem& s, const Frag<NC>& f, int kind) {
+  const bool rowkind = kind_rowwise(kind);
+  const bool negim = kind == A_DAG || kind == B_DAG;
+#pragma unroll
+  for (int i = 0; i < Shape<NC>::UPT; i++) {
+    int r, kc;
+    unit_rc<NC>(threadIdx.x + THREADS * i, rowkind, r, kc);
+    const float4 im = negim ? neg4(f.im[i]) : f.im[i];
+    if (kind == A_NORM || kind == A_DAG)
+      put_A<NC>(s, r, kc, f.re[i], im);
+    else
+      put_B<NC>(s, r, kc, f.re[i], im);
+  }
+}
+
+// ------------------------------------------------------------- MMA ----
+// D (TMEM column dcol) = X Y  (acc = 0) or += X Y (acc = 1): 2 parts x 3
+// split pairs x KS k-steps, then one commit to the barrier.  Thread 0 only.
+template <int NC>
+__device__ __forceinline__ void issue_product(const Smem& s, uint32_t dtmem, uint32_t acc) {
+  using SH = Shape<NC>;
+  constexpr uint32_t idesc = (1u << 4)                             // D: F32
+                             | (2u << 7) | (2u << 10)              // A, B: TF32
+                             | ((uint32_t)(NC >> 3) << 17)         // N = NC
+                             | ((uint32_t)((2 * NC) >> 4) << 24);  // M = 2 NC
+  const uint32_t a0 = saddr(s.A), b0 = saddr(s.B);
+  uint32_t first = 1;
+#pragma unroll
+  for (int part = 0; part < 2; part++) {
+    const uint32_t apart = part == 0 ? (NC / 8) * SH::SBO : 0u;  // [Xr; Xi] for Yr, [-Xi; Xr] for Yi
+#pragma unroll
+    for (int pr = 0; pr < 3; pr++) {
+      const uint32_t asplit = pr == 0 ? 1u : 0u;  // lo*hi, hi*lo, hi*hi
+      const uint32_t bsplit = pr == 1 ? 1u : 0u;
+      const uint32_t abase = a0 + asplit * SH::A_BYTES + apart;
+      const uint32_t bbase = b0 + (2u * part + bsplit) * SH::B_BYTES;
+#pragma unroll
+      for (int k = 0; k < SH::KS; k++) {
+        mma_tf32(dtmem, sdesc(abase + 2u * k * LBO, LBO, SH::SBO), sdesc(bbase + 2u * k * LBO, LBO, SH::SBO), idesc,
+                 first ? acc : 1u);
+        first = 0;
+      }
+    }
+  }
+  mma_commit(s.bar);
+}
+
+// ---------------------------------------------------------- per-thread ----
+// accumulator row (0..2NC-1) and column half this thread reads
+template <int NC>
+struct Role {
+  int rr, c0, m;
+  bool valid, im;
+  uint32_t lane;
+  __device__ Role() {
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31, q = w & 3;
+    c0 = (w >> 2) * Shape<NC>::HALF;
+    if (NC == 64) {
+      rr = 32 * q + l;
+      valid = true;
+    } else {
+      rr = 16 * q + l;
+      valid = l < 16;
+    }
+    im = rr >= NC;
+    m = im ? rr - NC : rr;
+    lane = (uint32_t)(32 * q) << 16;
+  }
+};
+
+// left operand from the accumulator row: X = D (scale 1) or, for the Horner
+// step, X = 1 + (i sc) D
+template <int NC>
+__device__ __forceinline__ void epi_A(const Smem& s, const Role<NC>& ro, const float* v, bool horner, float sc) {
+  if (!ro.valid) return;
+#pragma unroll
+  for (int q = 0; q < Shape<NC>::HALF / 4; q++) {
+    const int k0 = ro.c0 + 4 * q;
+    float4 x = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+    if (!horner) {
+      if (!ro.im) {
+        st4<NC>(s.A, Shape<NC>::A_BYTES, opoff<NC>(NC + ro.m, k0), x);
+      } else {
+        st4<NC>(s.A, Shape<NC>::A_BYTES, opoff<NC>(2 * NC + ro.m, k0), x);
+        st4<NC>(s.A, Shape<NC>::A_BYTES, opoff<NC>(ro.m, k0), neg4(x));
+      }
+    } else if (!ro.im) {  // Xi = sc Dr
+      const float4 y = make_float4(sc * x.x, sc * x.y, sc * x.z, sc * x.w);
+      st4<NC>(s.A, Shape<NC>::A_BYTES, opoff<NC>(2 * NC + ro.m, k0), y);
+      st4<NC>(s.A, Shape<NC>::A_BYTES, opoff<NC>(ro.m, k0), neg4(y));
+    } else {  // Xr = 1 - sc Di
+      float4 y = make_float4(-sc * x.x, -sc * x.y, -sc * x.z, -sc * x.w);
+      if (ro.m == k0) y.x += 1.f;
+      if (ro.m == k0 + 1) y.y += 1.f;
+      if (ro.m == k0 + 2) y.z += 1.f;
+      if (ro.m == k0 + 3) y.w += 1.f;
+      st4<NC>(s.A, Shape<NC>::A_BYTES, opoff<NC>(NC + ro.m, k0), y);
+    }
+  }
+}
+
+// left operand X = D^dag from the accumulator row (transposed stores)
+template <int NC>
+__device__ __forceinline__ void epi_A_dag(const Smem& s, const Role<NC>& ro, const float* v) {
+  if (!ro.valid) return;
+#pragma unroll
+  for (int c = 0; c < Shape<NC>::HALF; c++) {
+    const int j = ro.c0 + c;  // D[m][j] -> X[j][m]
+    if (!ro.im) {
+      st1<NC>(s.A, Shape<NC>::A_BYTES, opoff<NC>(NC + j, ro.m), v[c]);
+    } else {
+      st1<NC>(s.A, Shape<NC>::A_BYTES, opoff<NC>(2 * NC + j, ro.m), -v[c]);
+      st1<NC>(s.A, Shape<NC>::A_BYTES, opoff<NC>(j, ro.m), v[c]);
+    }
+  }
+}
+
+// right operand B = D (zmap = false) or B = 3/2 - D/2 (zmap = true) from the
+// accumulator row: Bs[j][m] = D[m][j] (transposed stores)
+template <int NC>
+__device__ __forceinline__ void epi_B(const Smem& s, const Role<NC>& ro, const float* v, bool zmap) {
+  if (!ro.valid) return;
+  unsigned char* base = s.B + (ro.im ? 2 * Shape<NC>::B_BYTES : 0);
+#pragma unroll
+  for (int c = 0; c < Shape<NC>::HALF; c++) {
+    const int j = ro.c0 + c;
+    float x = v[c];
+    if (zmap) x = (!ro.im && j == ro.m ? 1.5f : 0.f) - 0.5f * x;
+    st1<NC>(base, Shape<NC>::B_BYTES, opoff<NC>(j, ro.m), x);
+  }
+}
+
+// accumulator row -> plain tile (plane 0 real, plane 1 imaginary)
+template <int NC>
+__device__ __forceinline__ void epi_plain(const Smem& s, const Role<NC>& ro, const float* v) {
+  if (!ro.valid) return;
+  float* row = s.plain + ((ro.im ? NC : 0) + ro.m) * Shape<NC>::PS + ro.c0;
+#pragma unroll
+  for (int q = 0; q < Shape<NC>::HALF / 4; q++)
+    *reinterpret_cast<float4*>(row + 4 * q) = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+}
+
+// start an MMA on operands just written by all threads
+template <int NC>
+__device__ __forceinline__ void go(const Smem& s, uint32_t dtmem, uint32_t acc) {
+  fence_async_smem();
+  fence_before();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    fence_after();
+    issue_product<NC>(s, dtmem, acc);
+  }
+}
+
+// wait for the last committed product; CTA-uniform result
+__device__ __forceinline__ bool done(const Smem& s, uint32_t& phase) {
+  const bool ok = mbar_wait(s.bar, phase & 1u);
+  phase++;
+  const bool bad = __syncthreads_or(!ok);
+  fence_after();
+  return !bad;
+}
+
+// one staple term of the link (x, mu): first = X1 Y1, second += (X1 Y1) Y2
+struct Term {
+  const float2* a;
+  const float2* b1;
+  const float2* b2;
+  int ka, kb1, kb2;
+};
+
+template <int NC>
+__device__ __forceinline__ Term staple_term(const Lat& L, const float2* __restrict__ aos, int mu, int x, int i) {
+  const size_t NN = (size_t)NC * NC;
+  const int j = i >> 1;
+  const int nu = j < mu ? j : j + 1;
+  auto link = [&](int d, int site) { return aos + ((size_t)d * L.V + site) * NN; };
+  const int xpmu = nb_plus(L, mu, x);
+  Term t;
+  if ((i & 1) == 0) {  // upper: U_nu(x+mu) U_mu^dag(x+nu) U_nu^dag(x)
+    t.a = link(nu, xpmu);
+    t.ka = A_NORM;
+    t.b1 = link(mu, nb_plus(L, nu, x));
+    t.kb1 = B_DAG;
+    t.b2 = link(nu, x);
+    t.kb2 = B_DAG;
+  } else {  // lower: U_nu^dag(x+mu-nu) U_mu^dag(x-nu) U_nu(x-nu)
+    const int xmnu = nb_minus(L, nu, x);
+    t.a = link(nu, nb_minus(L, nu, xpmu));
+    t.ka = A_DAG;
+    t.b1 = link(mu, xmnu);
+    t.kb1 = B_DAG;
+    t.b2 = link(nu, xmnu);
+    t.kb2 = B_NORM;
+  }
+  return t;
+}
+
+// MODE 0: Pout = Pin - eps_k F(U)
+// MODE 1: also Uout = exp(i eps_d Pout) U (reunitarised when reunit)
+// MODE 2: Uout = exp(i eps_d Pin) U only
+// U is read from `aos` (per-link contiguous copy); Uout may be U itself.
+template <int NC, int MODE>
+__global__ void __launch_bounds__(THREADS, NC == 64 ? 1 : 2)
+    k_link(Lat L, const float2* __restrict__ aos, const float2* Pin, float2* Pout, float2* Uout, float eps_k,
+           float eps_d, int order, int reunit, unsigned* status) {
+  using SH = Shape<NC>;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  Smem s;
+  s.A = smem_raw;
+  s.B = smem_raw + 2 * SH::A_BYTES;
+  s.plain = reinterpret_cast<float*>(s.B + 4 * SH::B_BYTES);
+  s.bar = reinterpret_cast<uint64_t*>(smem_raw + 2 * SH::A_BYTES + 4 * SH::B_BYTES + SH::PLAIN_BYTES);
+  s.slot = reinterpret_cast<uint32_t*>(s.bar + 1);
+  const int tid = threadIdx.x;
+  if (tid == 0) mbar_init(s.bar);
+  if (tid < 32) tmem_alloc(s.slot, SH::TMEM_COLS);
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const uint32_t tbase = *s.slot;
+  const uint32_t tT = tbase, tS = tbase + NC;
+  const Role<NC> ro;
+  uint32_t phase = 0;
+  bool ok = true;
+  float v[SH::HALF];
+  const size_t NN = (size_t)NC * NC;
+  const long nl = (long)L.V * L.D;
+
+  for (long l = blockIdx.x; l < nl && ok; l += gridDim.x) {
+    const int mu = (int)(l / L.V);
+    const int x = (int)(l - (long)mu * L.V);
+    const float2* ulink = aos + ((size_t)mu * L.V + x) * NN;
+    const size_t fb = mbase(L, mu, x);
+    Frag<NC> fa, fb1;
+    if (MODE != 2) {
+      // ---- staple sum S (TMEM columns NC..2NC-1)
+      const int nterms = 2 * (L.D - 1);
+      Term t = staple_term<NC>(L, aos, mu, x, 0);
+      fetch<NC>(fa, t.a, kind_rowwise(t.ka));
+      fetch<NC>(fb1, t.b1, kind_rowwise(t.kb1));
+      for (int i = 0; i < nterms && ok; i++) {
+        put<NC>(s, fa, t.ka);
+        put<NC>(s, fb1, t.kb1);
+        go<NC>(s, tT, 0);
+        fetch<NC>(fb1, t.b2, kind_rowwise(t.kb2));
+        ok = done(s, phase);
+        if (!ok) break;
+        tmem_ld(tT + ro.lane + ro.c0, v);
+        epi_A<NC>(s, ro, v, false, 0.f);
+        put<NC>(s, fb1, t.kb2);
+        go<NC>(s, tS, i > 0 ? 1u : 0u);
+        if (i + 1 < nterms) {
+          t = staple_term<NC>(L, aos, mu, x, i + 1);
+          fetch<NC>(fa, t.a, kind_rowwise(t.ka));
+          fetch<NC>(fb1, t.b1, kind_rowwise(t.kb1));
+        } else {
+          fetch<NC>(fa, ulink, true);
+        }
+        ok = done(s, phase);
+      }
+      if (!ok) break;
+      // ---- W = U_mu(x) S  (TMEM columns 0..NC-1)
+      tmem_ld(tS + ro.lane + ro.c0, v);
+      epi_B<NC>(s, ro, v, false);
+      put<NC>(s, fa, A_NORM);
+      go<NC>(s, tT, 0);
+      float2 pn[SH::EPT];
+#pragma unroll
+      for (int q = 0; q < SH::EPT; q++) pn[q] = Pin[fb + 32 * (size_t)(tid + THREADS * q)];
+      ok = done(s, phase);
+      if (!ok) break;
+      tmem_ld(tT + ro.lane + ro.c0, v);
+      epi_plain<NC>(s, ro, v);
+      __syncthreads();
+      // ---- kick with the traceless anti-hermitian part of W
+      float trim = 0.f;
+      for (int k = 0; k < NC; k++) trim += s.plain[(NC + k) * SH::PS + k];
+      trim = trim / (float)NC;
+#pragma unroll
+      for (int q = 0; q < SH::EPT; q++) {
+        const int e = tid + THREADS * q;
+        const int r = e / NC, c = e % NC;
+        float fr, fi;
+        if (r == c) {
+          fr = s.plain[(NC + r) * SH::PS + r] - trim;
+          fi = 0.f;
+        } else {
+          fr = 0.5f * (s.plain[(NC + r) * SH::PS + c] + s.plain[(NC + c) * SH::PS + r]);
+          fi = -0.5f * (s.plain[r * SH::PS + c] - s.plain[c * SH::PS + r]);
+        }
+        pn[q].x = fmaf(-eps_k, fr, pn[q].x);
+        pn[q].y = fmaf(-eps_k, fi, pn[q].y);
+        Pout[fb + 32 * (size_t)e] = pn[q];
+      }
+      if (MODE == 0) continue;
+      __syncthreads();
+#pragma unroll
+      for (int q = 0; q < SH::EPT; q++) {
+        const int e = tid + THREADS * q;
+        s.plain[(e / NC) * SH::PS + e % NC] = pn[q].x;
+        s.plain[(NC + e / NC) * SH::PS + e % NC] = pn[q].y;
+      }
+      __syncthreads();
+    } else {
+#pragma unroll
+      for (int q = 0; q < SH::EPT; q++) {
+        const int e = tid + THREADS * q;
+        const float2 p = Pin[fb + 32 * (size_t)e];
+        s.plain[(e / NC) * SH::PS + e % NC] = p.x;
+        s.plain[(NC + e / NC) * SH::PS + e % NC] = p.y;
+      }
+      __syncthreads();
+    }
+    // ---- drift: E = 1 + (i eps/L) P, E <- 1 + (i eps/k) E P (k = L-1..1), U' = E U
+    {
+      const float sc0 = order > 0 ? eps_d / (float)order : 0.f;
+#pragma unroll
+      for (int i = 0; i < SH::UPT; i++) {
+        int m, kc;
+        unit_rc<NC>(tid + THREADS * i, true, m, kc);
+        const float4 pr = *reinterpret_cast<const float4*>(s.plain + m * SH::PS + 4 * kc);
+        const float4 pi = *reinterpret_cast<const float4*>(s.plain + (NC + m) * SH::PS + 4 * kc);
+        float4 er = make_float4(-sc0 * pi.x, -sc0 * pi.y, -sc0 * pi.z, -sc0 * pi.w);
+        if (m == 4 * kc) er.x += 1.f;
+        if (m == 4 * kc + 1) er.y += 1.f;
+        if (m == 4 * kc + 2) er.z += 1.f;
+        if (m == 4 * kc + 3) er.w += 1.f;
+        put_A<NC>(s, m, kc, er, make_float4(sc0 * pr.x, sc0 * pr.y, sc0 * pr.z, sc0 * pr.w));
+      }
+      if (order > 1) {
+#pragma unroll
+        for (int i = 0; i < SH::UPT; i++) {  // B = P: Bs[j][k] = P[k][j]
+          int j, kc;
+          unit_rc<NC>(tid + THREADS * i, false, j, kc);
+          const float* pr = s.plain + 4 * kc * SH::PS + j;
+          const float* pi = s.plain + (NC + 4 * kc) * SH::PS + j;
+          put_B<NC>(s, j, kc, make_float4(pr[0], pr[SH::PS], pr[2 * SH::PS], pr[3 * SH::PS]),
+                    make_float4(pi[0], pi[SH::PS], pi[2 * SH::PS], pi[3 * SH::PS]));
+        }
+      }
+      fetch<NC>(fa, ulink, false);  // B = U_mu(x) for the last product
+      for (int k = order - 1; k >= 1 && ok; k--) {
+        go<NC>(s, tT, 0);
+        ok = done(s, phase);
+        if (!ok) break;
+        tmem_ld(tT + ro.lane + ro.c0, v);
+        epi_A<NC>(s, ro, v, true, eps_d / (float)k);
+      }
+      if (!ok) break;
+      put<NC>(s, fa, B_NORM);
+      go<NC>(s, tT, 0);
+      ok = done(s, phase);
+      if (!ok) break;
+      tmem_ld(tT + ro.lane + ro.c0, v);
+    }
+    if (reunit) {
+      // Newton-Schulz polar step: Y = U'^dag U', U'' = U' (3 - Y)/2
+      epi_A_dag<NC>(s, ro, v);
+      epi_B<NC>(s, ro, v, false);
+      go<NC>(s, tS, 0);
+      ok = done(s, phase);
+      if (!ok) break;
+      float y[SH::HALF];
+      tmem_ld(tS + ro.lane + ro.c0, y);
+      epi_B<NC>(s, ro, y, true);
+      epi_A<NC>(s, ro, v, false, 0.f);
+      go<NC>(s, tT, 0);
+      ok = done(s, phase);
+      if (!ok) break;
+      tmem_ld(tT + ro.lane + ro.c0, v);
+    }
+    epi_plain<NC>(s, ro, v);
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < SH::EPT; q++) {
+      const int e = tid + THREADS * q;
+      Uout[fb + 32 * (size_t)e] =
+          make_float2(s.plain[(e / NC) * SH::PS + e % NC], s.plain[(NC + e / NC) * SH::PS + e % NC]);
+    }
+    __syncthreads();
+  }
+
+  if (!ok) {
+    if (tid == 0) atomicOr(status, 1u);
+    // a product that has not completed still owns the accumulator: give it
+    // one more bounded wait before the columns are released
+    mbar_wait(s.bar, (phase - 1) & 1u);
+  }
+  fence_before();
+  __syncthreads();
+  if (tid < 32) {
+    fence_after();
+    tmem_dealloc(tbase, SH::TMEM_COLS);
+  }
+}
+
+// blocked field layout -> per-link contiguous row-major copy (32 sites x 32
+// elements per tile, both sides coalesced)
+static __global__ void k_to_aos(Lat L, const float2* __restrict__ f, float2* __restrict__ aos) {
+  __shared__ float2 tile[32][33];
+  const int b = blockIdx.x, d = blockIdx.y;
+  const int nn = L.N * L.N;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int chunks = (nn + 31) / 32;
+  for (int ch = blockIdx.z; ch < chunks; ch += gridDim.z) {
+    const int e0 = ch * 32;
+    for (int r = w; r < 32; r += 8) {
+      const int e = e0 + r;
+      if (e < nn) tile[r][lane] = f[(((size_t)d * L.B + b) * nn + e) * 32 + lane];
+    }
+    __syncthreads();
+    for (int r = w; r < 32; r += 8) {
+      const int site = b * 32 + r, e = e0 + lane;
+      if (site < L.V && e < nn) aos[((size_t)d * L.V + site) * nn + e] = tile[lane][r];
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace tc
+}  // namespace askja

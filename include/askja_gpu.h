@@ -65,7 +65,8 @@ typedef struct {
   int precision;       /* ASKJA_FP64 or ASKJA_FP32 */
   int reunitarise;     /* -1 default (on for FP32, off for FP64), 0 off, 1 on */
   int device;          /* CUDA device ordinal */
-  int kernel_path;     /* 0 automatic; 1 row-per-thread kernels for every NC (testing) */
+  int kernel_path;     /* 0 automatic; 1 row-per-thread kernels for every NC (testing);
+                          2 tensor cores (FP32 with NC = 32 or 64 and DIM >= 2 only) */
   uint64_t seed;       /* Philox key for momenta, Metropolis uniforms and hot start */
 } askja_params;
 
@@ -155,10 +156,12 @@ ASKJA_API int askja_md_steps(askja_ctx* ctx, int nsteps, double eps);
 /* ---- autotuning (not in the reference) ---------------------------------- */
 /* Kernel mapping for the force / link-update kernel of one (NC, DIM,
  * precision): thread-per-link (NC <= 4, all matrices in registers) or
- * row-per-thread (NC threads per link, shared-memory tiles), the number of
- * sites per CTA of the latter, and the register budget of the former. */
+ * row-per-thread (NC threads per link, shared-memory tiles) or tensor cores
+ * (FP32, NC = 32 or 64: every complex product a split-TF32 MMA), the number
+ * of sites per CTA of the row kernels, and the register budget of the
+ * thread-per-link kernels. */
 typedef struct {
-  int path;       /* 0 thread-per-link, 1 row-per-thread */
+  int path;       /* 0 thread-per-link, 1 row-per-thread, 2 tensor cores */
   int groups;     /* row-per-thread: sites per CTA (0 = default) */
   int occupancy;  /* thread-per-link: 0 default registers, 1 tighter budget / more CTAs */
   int ncand;      /* candidates timed */
