@@ -221,8 +221,17 @@ cudaError_t reunit(const LaunchCtx& c, void* U) {
 template <typename T>
 cudaError_t plaq(const LaunchCtx& c, const void* U, double* partial, double* out) {
   using S2 = typename Storage<T>::type;
-  const unsigned nb = blocks_for(c.lat.V, misc::RED_THREADS);
   const int N = c.lat.N;
+  if (N >= misc::BIG_NC) {
+    auto k = misc::k_plaq_big<S2>;
+    const size_t smem = 2 * (size_t)N * (N + 1) * sizeof(cpx<double>);
+    cudaError_t e;
+    if ((e = set_smem(k, smem)) != cudaSuccess) return e;
+    k<<<c.lat.V, misc::RED_THREADS, smem, c.stream>>>(c.lat, (const S2*)U, partial);
+    misc::k_finish<2><<<1, misc::RED_THREADS, 0, c.stream>>>(partial, c.lat.V, out);
+    return cudaGetLastError();
+  }
+  const unsigned nb = blocks_for(c.lat.V, misc::RED_THREADS);
   if (N == 2)
     misc::k_plaq<2, S2><<<nb, misc::RED_THREADS, 0, c.stream>>>(c.lat, (const S2*)U, partial);
   else if (N == 3)
@@ -238,8 +247,14 @@ cudaError_t plaq(const LaunchCtx& c, const void* U, double* partial, double* out
 template <typename T>
 cudaError_t linksums(const LaunchCtx& c, const void* Pa, const void* Pb, const void* U, double* partial, double* out) {
   using S2 = typename Storage<T>::type;
-  const unsigned nb = blocks_for(nlinks(c.lat), misc::RED_THREADS);
   const int N = c.lat.N;
+  if (N >= misc::BIG_NC) {
+    misc::k_linksums_big<S2><<<(unsigned)nlinks(c.lat), misc::RED_THREADS, 0, c.stream>>>(
+        c.lat, (const S2*)Pa, (const S2*)Pb, (const S2*)U, partial);
+    misc::k_finish<3><<<1, misc::RED_THREADS, 0, c.stream>>>(partial, (int)nlinks(c.lat), out);
+    return cudaGetLastError();
+  }
+  const unsigned nb = blocks_for(nlinks(c.lat), misc::RED_THREADS);
   if (N == 2)
     misc::k_linksums<2, S2><<<nb, misc::RED_THREADS, 0, c.stream>>>(c.lat, (const S2*)Pa, (const S2*)Pb,
                                                                     (const S2*)U, partial);
@@ -292,6 +307,11 @@ template <typename T>
 cudaError_t refresh(const LaunchCtx& c, void* P, uint64_t seed, const unsigned long long* traj_dev,
                     unsigned long long traj_host, double scale) {
   using S2 = typename Storage<T>::type;
+  if (c.lat.N >= misc::BIG_NC) {
+    misc::k_refresh_big<S2><<<(unsigned)nlinks(c.lat), misc::RED_THREADS, 0, c.stream>>>(c.lat, (S2*)P, seed, traj_dev,
+                                                                                         traj_host, scale);
+    return cudaGetLastError();
+  }
   misc::k_refresh<S2><<<blocks_for(nlinks(c.lat), 128), 128, 0, c.stream>>>(c.lat, (S2*)P, seed, traj_dev, traj_host,
                                                                               scale);
   return cudaGetLastError();

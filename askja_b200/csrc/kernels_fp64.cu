@@ -12,7 +12,9 @@ size_t partial_doubles(const Lat& L) {
   const size_t links = 3 * ((nl + misc::RED_THREADS - 1) / misc::RED_THREADS);
   const size_t gauss =
       2 * (size_t)L.N * L.N * ((nl + detail::GAUSS_LINKS_PER_BLOCK - 1) / detail::GAUSS_LINKS_PER_BLOCK);
-  return std::max(plaq, std::max(links, gauss)) + 64;
+  // one partial per site / per link for the large-NC reductions
+  const size_t big = L.N >= misc::BIG_NC ? std::max(2 * (size_t)L.V, 3 * (size_t)nl) : 0;
+  return std::max(std::max(plaq, big), std::max(links, gauss)) + 64;
 }
 
 int rows_effective_groups(int N, bool fp64, int want) {

@@ -491,5 +491,180 @@ static __global__ void k_count_nonfinite(const double* __restrict__ x, long n, u
   if (c) atomicAdd(count, c);
 }
 
+// ---- large colour number (NC >= BIG_NC): one CTA per site or per link ----
+// The thread-per-site / thread-per-link kernels above carry O(NC^3) / O(NC^2)
+// serial work per thread, which leaves a lattice of a few thousand sites with
+// a few thousand threads; these spread one site or link over a CTA.
+
+constexpr int BIG_NC = 16;
+
+// Plaquette sums of one site (same sums as plaq_site): B = U_nu(x+mu) and
+// C = U_mu(x+nu) staged in shared memory as FP64 ([N][N+1]), thread t owns row
+// t / 4 and the columns j = 4q + t % 4 of AB and DC (A = U_mu(x), D = U_nu(x)
+// read from global), tr = sum Re (AB)_ij conj((DC)_ij); partial[s*2 + {0,1}].
+template <typename S2>
+__global__ void __launch_bounds__(RED_THREADS) k_plaq_big(Lat L, const S2* __restrict__ U, double* __restrict__ partial) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int N = L.N, NP = N + 1;
+  cpx<double>* Bs = reinterpret_cast<cpx<double>*>(smem_raw);
+  cpx<double>* Cs = Bs + N * NP;
+  const int s = blockIdx.x;
+  const int tid = threadIdx.x;
+  const int rows_per_pass = RED_THREADS / 4;
+  double trt = 0.0, trs = 0.0;
+  int nt = 0, ns = 0;
+  for (int mu = 0; mu < L.D; mu++) {
+    const int xpmu = nb_plus(L, mu, s);
+    for (int nu = mu + 1; nu < L.D; nu++) {
+      const int xpnu = nb_plus(L, nu, s);
+      __syncthreads();
+      for (int e = tid; e < N * N; e += RED_THREADS) {
+        const int r = e / N, c = e - (e / N) * N;
+        Bs[r * NP + c] = ldc<double>(U + eoff(L, nu, e, xpmu));
+        Cs[r * NP + c] = ldc<double>(U + eoff(L, mu, e, xpnu));
+      }
+      __syncthreads();
+      double tr = 0.0;
+      for (int i0 = 0; i0 < N; i0 += rows_per_pass) {
+        const int i = i0 + tid / 4;
+        if (i >= N) continue;
+        cpx<double> ab[16], dc[16];
+#pragma unroll
+        for (int q = 0; q < 16; q++) ab[q] = dc[q] = czero<double>();
+        for (int k = 0; k < N; k++) {
+          const cpx<double> a = ldc<double>(U + eoff(L, mu, i * N + k, s));
+          const cpx<double> d = ldc<double>(U + eoff(L, nu, i * N + k, s));
+#pragma unroll
+          for (int q = 0; q < 16; q++) {
+            const int j = 4 * q + (tid & 3);
+            if (j < N) {
+              cmac(ab[q], a, Bs[k * NP + j]);
+              cmac(dc[q], d, Cs[k * NP + j]);
+            }
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < 16; q++) {
+          tr = fma(ab[q].re, dc[q].re, tr);
+          tr = fma(ab[q].im, dc[q].im, tr);
+        }
+      }
+      if (mu == 0) {
+        trt += tr;
+        nt++;
+      } else {
+        trs += tr;
+        ns++;
+      }
+    }
+  }
+  double v[2] = {trt, trs};
+  block_sum<2>(v);
+  if (tid == 0) {
+    partial[(size_t)s * 2 + 0] = nt - v[0] / N;
+    partial[(size_t)s * 2 + 1] = ns - v[1] / N;
+  }
+}
+
+// link_sums of one link per CTA; partial[t*3 + k]
+template <typename S2>
+__global__ void __launch_bounds__(RED_THREADS) k_linksums_big(Lat L, const S2* __restrict__ Pa,
+                                                              const S2* __restrict__ Pb, const S2* __restrict__ U,
+                                                              double* __restrict__ partial) {
+  const int N = L.N;
+  const long t = blockIdx.x;
+  const int d = (int)(t / L.V);
+  const int s = (int)(t - (long)d * L.V);
+  double a = 0.0, b = 0.0, c = 0.0;
+  for (int e = threadIdx.x; e < N * N; e += RED_THREADS) {
+    const int i = e / N, j = e - (e / N) * N;
+    if (Pa) {
+      const cpx<double> x = ldc<double>(Pa + eoff(L, d, i * N + j, s));
+      const cpx<double> y = ldc<double>(Pa + eoff(L, d, j * N + i, s));
+      a = fma(x.re, y.re, a);
+      a = fma(-x.im, y.im, a);
+      if (Pb) {
+        const cpx<double> x2 = ldc<double>(Pb + eoff(L, d, i * N + j, s));
+        const cpx<double> y2 = ldc<double>(Pb + eoff(L, d, j * N + i, s));
+        b = fma(x.re + x2.re, y.re + y2.re, b);
+        b = fma(-(x.im + x2.im), y.im + y2.im, b);
+      }
+    }
+    if (U) {
+      cpx<double> aij = czero<double>(), aji = czero<double>();
+      for (int k = 0; k < N; k++) {
+        cmac_nc(aij, ldc<double>(U + eoff(L, d, i * N + k, s)), ldc<double>(U + eoff(L, d, j * N + k, s)));
+        cmac_nc(aji, ldc<double>(U + eoff(L, d, j * N + k, s)), ldc<double>(U + eoff(L, d, i * N + k, s)));
+      }
+      if (i == j) {
+        aij.re -= 1.0;
+        aji.re -= 1.0;
+      }
+      c = fma(aij.re, aji.re, c);
+      c = fma(-aij.im, aji.im, c);
+    }
+  }
+  double v[3] = {a, 0.25 * b, c};
+  block_sum<3>(v);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int k = 0; k < 3; k++) partial[(size_t)t * 3 + k] = v[k];
+}
+
+// refresh_link with one CTA per link: thread per off-diagonal pair (the pair's
+// two normals come from one Philox block), the diagonal by thread 0 in the
+// same order as refresh_link, so the momenta are identical.
+template <typename S2>
+__global__ void k_refresh_big(Lat L, S2* __restrict__ P, uint64_t seed, const unsigned long long* __restrict__ traj_dev,
+                              unsigned long long traj_host, double scale) {
+  const uint32_t traj = (uint32_t)(traj_dev ? *traj_dev : traj_host);
+  const int N = L.N;
+  const long t = blockIdx.x;
+  const int d = (int)(t / L.V);
+  const int s = (int)(t - (long)d * L.V);
+  const unsigned long long lk = (unsigned long long)s * L.D + d;
+  const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+  auto block = [&](int blk, double (&g)[4]) {
+    u32x4 c;
+    c.x = (uint32_t)blk;
+    c.y = (uint32_t)lk;
+    c.z = (uint32_t)(lk >> 32);
+    c.w = traj;
+    normals4(philox4x32_10(c, k0, k1), g);
+  };
+  for (int e = threadIdx.x; e < N * N; e += blockDim.x) {
+    const int i = e / N, j = e - (e / N) * N;
+    if (j <= i) continue;
+    const int p = i * (2 * N - i - 1) / 2 + (j - i - 1);
+    double g[4];
+    block((2 * p) >> 2, g);
+    const double xs = g[(2 * p) & 3], xa = g[(2 * p + 1) & 3];
+    stc(P + eoff(L, d, i * N + j, s), mkc<double>(0.5 * scale * xs, -0.5 * scale * xa));
+    stc(P + eoff(L, d, j * N + i, s), mkc<double>(0.5 * scale * xs, 0.5 * scale * xa));
+  }
+  if (threadIdx.x == 0) {
+    const int a0 = N * (N - 1);
+    int cur = -1;
+    double g[4];
+    double suffix = 0.0;
+    for (int dd = N - 1; dd >= 0; dd--) {
+      double val = suffix;
+      if (dd >= 1) {
+        const int m = dd - 1;
+        const double nm = sqrt(0.5 / ((double)(m + 1) * (m + 2)));
+        const int a = a0 + m;
+        if ((a >> 2) != cur) {
+          block(a >> 2, g);
+          cur = a >> 2;
+        }
+        const double xm = g[a & 3];
+        val -= dd * nm * xm;
+        suffix += nm * xm;
+      }
+      stc(P + eoff(L, d, dd * N + dd, s), mkc<double>(scale * val, 0.0));
+    }
+  }
+}
+
 }  // namespace misc
 }  // namespace askja

@@ -15,8 +15,13 @@
 // column c in TMEM column c.
 //
 // Precision: split TF32 x 3 with FP32 accumulation.  Every operand x is
-// stored as hi = tf32(x) and lo = tf32(x - hi); each product accumulates
-// lo*hi + hi*lo + hi*hi (the lo*lo term, ~2^-22 relative, is dropped).
+// stored as hi = tf32(x) and lo = tf32(x - hi); each product takes hi*hi into
+// a main accumulator and lo*hi + hi*lo (~2^-11 smaller) into a second one,
+// and the epilogue adds the two with one round-to-nearest; the lo*lo term,
+// ~2^-22 relative, is dropped.  The accumulation inside the tensor core is
+// not unbiased (without reunitarisation the link norms drift by ~1e-6 per
+// update); keeping the small terms out of the large accumulator halves that
+// drift, and the Newton-Schulz step below removes it after every update.
 //
 // Shared-memory operand layout: the K-major no-swizzle canonical layout of
 // the tcgen05 matrix descriptors -- 8 rows x 16 bytes core matrices; the
@@ -26,8 +31,9 @@
 //
 // One CTA (256 threads = 8 warps) owns one link at a time and walks the
 // links of the lattice with a grid stride.  Thread 0 issues the MMAs and
-// commits them to one mbarrier; all threads wait on it (bounded: after about
-// a second the kernel records an error in *status and stops), read the
+// commits them to one mbarrier; one thread polls it while the others wait in
+// the CTA barrier (bounded: after about a second the kernel records an error
+// in *status and stops), then all threads read the
 // accumulator with tcgen05.ld (warp w reads TMEM lanes 32(w%4).., columns
 // (w/4)*NC/2 ..), and write the next operand.  Neighbour links are read from
 // a per-link contiguous copy of U (k_to_aos), P and the outputs use the
@@ -55,10 +61,13 @@ struct Shape {
   static constexpr uint32_t SBO = KC * LBO;
   static constexpr uint32_t A_BYTES = (3 * NC / 8) * SBO;  // one split of the triple block
   static constexpr uint32_t B_BYTES = (NC / 8) * SBO;      // one split of one part
-  static constexpr int PS = NC + 4;                         // plain tile row stride (floats)
+  static constexpr int PS = NC + 1;  // plain tile row stride (floats): odd, so rows and columns are conflict-free
   static constexpr uint32_t PLAIN_BYTES = 2u * NC * PS * 4;
   static constexpr uint32_t SMEM = 2 * A_BYTES + 4 * B_BYTES + PLAIN_BYTES + 32;
-  static constexpr int TMEM_COLS = 2 * NC;  // T at column 0, S at column NC
+  // main (hi*hi) accumulators T at column 0 and S at NC; the cross-term
+  // accumulators of each at +2NC
+  static constexpr int TMEM_COLS = 4 * NC;
+  static constexpr uint32_t CORR = 2 * NC;
   static constexpr int UPT = NC * NC / 4 / THREADS;  // 4-element units per thread
   static constexpr int EPT = NC * NC / THREADS;      // elements per thread
   static constexpr int HALF = NC / 2;                // accumulator columns per thread
@@ -82,12 +91,14 @@ __device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// bounded wait: false after ~2^31 clock cycles (about a second)
+// bounded wait: false after ~2^31 clock cycles (about a second); the clock is
+// read once every 64 polls
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
   const long long t0 = clock64();
-  while (!mbar_try(bar, parity))
-    if (clock64() - t0 > (1LL << 31)) return false;
-  return true;
+  for (uint32_t n = 1;; n++) {
+    if (mbar_try(bar, parity)) return true;
+    if ((n & 63u) == 0 && clock64() - t0 > (1LL << 31)) return false;
+  }
 }
 
 __device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
@@ -165,14 +176,16 @@ __device__ __forceinline__ void tmem_ld(uint32_t taddr, float (&v)[32]) {
   for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
 }
 
+// round to the 10-bit TF32 mantissa, ties away from zero, on the integer
+// pipes (IEEE sign-magnitude: adding half a TF32 ulp to the magnitude bits
+// and clearing the 13 dropped bits rounds the magnitude); a conversion
+// instruction per element would saturate the XU pipe
 __device__ __forceinline__ float tf32r(float x) {
-  uint32_t h;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(x));
-  return __uint_as_float(h);
+  return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
 }
 __device__ __forceinline__ void split(float x, float& hi, float& lo) {
   hi = tf32r(x);
-  lo = tf32r(x - hi);
+  lo = tf32r(__fsub_rn(x, hi));
 }
 
 // ------------------------------------------------------------ layout ----
@@ -291,8 +304,10 @@ __device__ __forceinline__ void put(const Smem& s, const Frag<NC>& f, int kind) 
 }
 
 // ------------------------------------------------------------- MMA ----
-// D (TMEM column dcol) = X Y  (acc = 0) or += X Y (acc = 1): 2 parts x 3
-// split pairs x KS k-steps, then one commit to the barrier.  Thread 0 only.
+// D = X Y (acc = 0) or D += X Y (acc = 1): 2 parts x 3 split pairs x KS
+// k-steps, hi*hi into the main accumulator at dtmem, lo*hi and hi*lo into
+// the cross-term accumulator at dtmem + CORR; then one commit to the
+// barrier.  Thread 0 only.
 template <int NC>
 __device__ __forceinline__ void issue_product(const Smem& s, uint32_t dtmem, uint32_t acc) {
   using SH = Shape<NC>;
@@ -300,8 +315,10 @@ __device__ __forceinline__ void issue_product(const Smem& s, uint32_t dtmem, uin
                              | (2u << 7) | (2u << 10)              // A, B: TF32
                              | ((uint32_t)(NC >> 3) << 17)         // N = NC
                              | ((uint32_t)((2 * NC) >> 4) << 24);  // M = 2 NC
-  const uint32_t a0 = saddr(s.A), b0 = saddr(s.B);
-  uint32_t first = 1;
+  // the start address is the low 14-bit field (address / 16) and every
+  // operand lies below 256 KB, so offsets are added to the descriptor directly
+  const uint64_t da = sdesc(saddr(s.A), LBO, SH::SBO), db = sdesc(saddr(s.B), LBO, SH::SBO);
+  uint32_t first_main = 1, first_corr = 1;
 #pragma unroll
   for (int part = 0; part < 2; part++) {
     const uint32_t apart = part == 0 ? (NC / 8) * SH::SBO : 0u;  // [Xr; Xi] for Yr, [-Xi; Xr] for Yi
@@ -309,13 +326,18 @@ __device__ __forceinline__ void issue_product(const Smem& s, uint32_t dtmem, uin
     for (int pr = 0; pr < 3; pr++) {
       const uint32_t asplit = pr == 0 ? 1u : 0u;  // lo*hi, hi*lo, hi*hi
       const uint32_t bsplit = pr == 1 ? 1u : 0u;
-      const uint32_t abase = a0 + asplit * SH::A_BYTES + apart;
-      const uint32_t bbase = b0 + (2u * part + bsplit) * SH::B_BYTES;
+      const uint32_t aoff = asplit * SH::A_BYTES + apart;
+      const uint32_t boff = (2u * part + bsplit) * SH::B_BYTES;
+      const bool main = pr == 2;
+      const uint32_t d = main ? dtmem : dtmem + SH::CORR;
 #pragma unroll
       for (int k = 0; k < SH::KS; k++) {
-        mma_tf32(dtmem, sdesc(abase + 2u * k * LBO, LBO, SH::SBO), sdesc(bbase + 2u * k * LBO, LBO, SH::SBO), idesc,
-                 first ? acc : 1u);
-        first = 0;
+        const uint32_t f = main ? first_main : first_corr;
+        mma_tf32(d, da + ((aoff + 2u * k * LBO) >> 4), db + ((boff + 2u * k * LBO) >> 4), idesc, f ? acc : 1u);
+        if (main)
+          first_main = 0;
+        else
+          first_corr = 0;
       }
     }
   }
@@ -407,14 +429,27 @@ __device__ __forceinline__ void epi_B(const Smem& s, const Role<NC>& ro, const f
   }
 }
 
+// this thread's accumulator row: main + cross-term accumulator, one
+// round-to-nearest addition (taddr: main accumulator + lane + column)
+template <int NC>
+__device__ __forceinline__ void acc_row(uint32_t taddr, float (&v)[Shape<NC>::HALF]) {
+#pragma unroll
+  for (int h = 0; h < Shape<NC>::HALF; h += 16) {
+    float a[16], b[16];
+    tmem_ld(taddr + h, a);
+    tmem_ld(taddr + Shape<NC>::CORR + h, b);
+#pragma unroll
+    for (int i = 0; i < 16; i++) v[h + i] = __fadd_rn(a[i], b[i]);
+  }
+}
+
 // accumulator row -> plain tile (plane 0 real, plane 1 imaginary)
 template <int NC>
 __device__ __forceinline__ void epi_plain(const Smem& s, const Role<NC>& ro, const float* v) {
   if (!ro.valid) return;
   float* row = s.plain + ((ro.im ? NC : 0) + ro.m) * Shape<NC>::PS + ro.c0;
 #pragma unroll
-  for (int q = 0; q < Shape<NC>::HALF / 4; q++)
-    *reinterpret_cast<float4*>(row + 4 * q) = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+  for (int q = 0; q < Shape<NC>::HALF; q++) row[q] = v[q];
 }
 
 // start an MMA on operands just written by all threads
@@ -429,9 +464,11 @@ __device__ __forceinline__ void go(const Smem& s, uint32_t dtmem, uint32_t acc) 
   }
 }
 
-// wait for the last committed product; CTA-uniform result
+// wait for the last committed product; CTA-uniform result.  One thread polls
+// the barrier, the others sleep in the CTA barrier behind it.
 __device__ __forceinline__ bool done(const Smem& s, uint32_t& phase) {
-  const bool ok = mbar_wait(s.bar, phase & 1u);
+  bool ok = true;
+  if (threadIdx.x == 32) ok = mbar_wait(s.bar, phase & 1u);
   phase++;
   const bool bad = __syncthreads_or(!ok);
   fence_after();
@@ -478,7 +515,7 @@ __device__ __forceinline__ Term staple_term(const Lat& L, const float2* __restri
 // MODE 2: Uout = exp(i eps_d Pin) U only
 // U is read from `aos` (per-link contiguous copy); Uout may be U itself.
 template <int NC, int MODE>
-__global__ void __launch_bounds__(THREADS, NC == 64 ? 1 : 2)
+__global__ void __launch_bounds__(THREADS, NC == 64 ? 1 : 3)
     k_link(Lat L, const float2* __restrict__ aos, const float2* Pin, float2* Pout, float2* Uout, float eps_k,
            float eps_d, int order, int reunit, unsigned* status) {
   using SH = Shape<NC>;
@@ -523,7 +560,7 @@ __global__ void __launch_bounds__(THREADS, NC == 64 ? 1 : 2)
         fetch<NC>(fb1, t.b2, kind_rowwise(t.kb2));
         ok = done(s, phase);
         if (!ok) break;
-        tmem_ld(tT + ro.lane + ro.c0, v);
+        acc_row<NC>(tT + ro.lane + ro.c0, v);
         epi_A<NC>(s, ro, v, false, 0.f);
         put<NC>(s, fb1, t.kb2);
         go<NC>(s, tS, i > 0 ? 1u : 0u);
@@ -538,7 +575,7 @@ __global__ void __launch_bounds__(THREADS, NC == 64 ? 1 : 2)
       }
       if (!ok) break;
       // ---- W = U_mu(x) S  (TMEM columns 0..NC-1)
-      tmem_ld(tS + ro.lane + ro.c0, v);
+      acc_row<NC>(tS + ro.lane + ro.c0, v);
       epi_B<NC>(s, ro, v, false);
       put<NC>(s, fa, A_NORM);
       go<NC>(s, tT, 0);
@@ -547,7 +584,7 @@ __global__ void __launch_bounds__(THREADS, NC == 64 ? 1 : 2)
       for (int q = 0; q < SH::EPT; q++) pn[q] = Pin[fb + 32 * (size_t)(tid + THREADS * q)];
       ok = done(s, phase);
       if (!ok) break;
-      tmem_ld(tT + ro.lane + ro.c0, v);
+      acc_row<NC>(tT + ro.lane + ro.c0, v);
       epi_plain<NC>(s, ro, v);
       __syncthreads();
       // ---- kick with the traceless anti-hermitian part of W
@@ -596,8 +633,10 @@ __global__ void __launch_bounds__(THREADS, NC == 64 ? 1 : 2)
       for (int i = 0; i < SH::UPT; i++) {
         int m, kc;
         unit_rc<NC>(tid + THREADS * i, true, m, kc);
-        const float4 pr = *reinterpret_cast<const float4*>(s.plain + m * SH::PS + 4 * kc);
-        const float4 pi = *reinterpret_cast<const float4*>(s.plain + (NC + m) * SH::PS + 4 * kc);
+        const float* rp = s.plain + m * SH::PS + 4 * kc;
+        const float* ip = s.plain + (NC + m) * SH::PS + 4 * kc;
+        const float4 pr = make_float4(rp[0], rp[1], rp[2], rp[3]);
+        const float4 pi = make_float4(ip[0], ip[1], ip[2], ip[3]);
         float4 er = make_float4(-sc0 * pi.x, -sc0 * pi.y, -sc0 * pi.z, -sc0 * pi.w);
         if (m == 4 * kc) er.x += 1.f;
         if (m == 4 * kc + 1) er.y += 1.f;
@@ -621,7 +660,7 @@ __global__ void __launch_bounds__(THREADS, NC == 64 ? 1 : 2)
         go<NC>(s, tT, 0);
         ok = done(s, phase);
         if (!ok) break;
-        tmem_ld(tT + ro.lane + ro.c0, v);
+        acc_row<NC>(tT + ro.lane + ro.c0, v);
         epi_A<NC>(s, ro, v, true, eps_d / (float)k);
       }
       if (!ok) break;
@@ -629,7 +668,7 @@ __global__ void __launch_bounds__(THREADS, NC == 64 ? 1 : 2)
       go<NC>(s, tT, 0);
       ok = done(s, phase);
       if (!ok) break;
-      tmem_ld(tT + ro.lane + ro.c0, v);
+      acc_row<NC>(tT + ro.lane + ro.c0, v);
     }
     if (reunit) {
       // Newton-Schulz polar step: Y = U'^dag U', U'' = U' (3 - Y)/2
@@ -639,13 +678,13 @@ __global__ void __launch_bounds__(THREADS, NC == 64 ? 1 : 2)
       ok = done(s, phase);
       if (!ok) break;
       float y[SH::HALF];
-      tmem_ld(tS + ro.lane + ro.c0, y);
+      acc_row<NC>(tS + ro.lane + ro.c0, y);
       epi_B<NC>(s, ro, y, true);
       epi_A<NC>(s, ro, v, false, 0.f);
       go<NC>(s, tT, 0);
       ok = done(s, phase);
       if (!ok) break;
-      tmem_ld(tT + ro.lane + ro.c0, v);
+      acc_row<NC>(tT + ro.lane + ro.c0, v);
     }
     epi_plain<NC>(s, ro, v);
     __syncthreads();

@@ -43,10 +43,17 @@ CONFIGS = {
     "su3_32": dict(nc=3, dims=[32, 32, 32, 32], beta=6.0, dt=0.02, level=6, nsteps=50),
     "su8_10": dict(nc=8, dims=[10, 10, 10, 10], beta=20.0, dt=0.01, level=8, nsteps=100),
     "su3_8": dict(nc=3, dims=[8, 8, 8, 8], beta=5.70, dt=0.02, level=8, nsteps=50),
+    # large NC: every complex product of the FP32 path on the tensor cores (split TF32 x 3);
+    # the CPU sample runs the same colour number on a smaller lattice (per-link rates)
+    "su32_8": dict(nc=32, dims=[8, 8, 8, 8], beta=2048.0, dt=0.005, level=8, nsteps=20, tensor=True,
+                   cpu_dims=[2, 2, 2, 2]),
+    "su64_4x16": dict(nc=64, dims=[4, 16, 16], beta=8192.0, dt=0.005, level=8, nsteps=20, tensor=True,
+                      cpu_dims=[2, 2, 4]),
 }
 
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
+FALLBACK_BF16_TFLOPS = 1590.0
 
 
 def peaks():
@@ -56,6 +63,30 @@ def peaks():
         return float(p["hbm_gbs"]), "measured"
     except Exception:
         return FALLBACK_HBM_GBS, "fallback"
+
+
+def tf32_peak():
+    """Dense TF32 tensor peak: half the measured dense BF16 GEMM rate (the
+    tensor cores run TF32 at half the BF16 rate)."""
+    try:
+        with open(PEAKS_PATH) as f:
+            return 0.5 * float(json.load(f)["bf16_tflops"]), "measured bf16 / 2"
+    except Exception:
+        return 0.5 * FALLBACK_BF16_TFLOPS, "fallback bf16 / 2"
+
+
+def tensor_products_per_link(dim, level, reunit=True):
+    """Complex NC x NC products of one fused kick+drift link update on the
+    tensor path: 4(D-1) staple products, U S, LEVEL-1 Horner products, E U
+    and two Newton-Schulz products."""
+    order = level if 0 <= level <= 8 else 8
+    return 4 * (dim - 1) + 1 + max(order - 1, 0) + 1 + (2 if reunit else 0)
+
+
+def tensor_flops_per_link(nc, dim, level, reunit=True):
+    """Real MMA flops of one link update on the tensor path: every complex
+    product is 2 parts x 3 split pairs of an M=2NC, N=NC, K=NC real MMA."""
+    return tensor_products_per_link(dim, level, reunit) * 6 * 2 * (2 * nc) * nc * nc
 
 
 class Clocks:
@@ -245,8 +276,24 @@ def run_ours(args):
     bytes_per_lu = 4 * nc * nc * s
     achieved = bytes_per_lu * links / (f32["kernel_ms"] / 1e3) / 1e9
     traffic = measured_traffic(args.config)
+    if cfg.get("tensor"):
+        fpl = tensor_flops_per_link(nc, len(dims), cfg["level"])
+        sec = f32["kernel_ms"] / 1e3
+        pk, src = tf32_peak()
+        tflops = fpl * links / sec / 1e12
+        roofline = {"bound": "tensor", "kernel": f"tensor-core link update (tc::k_link<{nc},1> + per-link copy of U)",
+                    "achieved": tflops, "peak": pk, "unit": "TFLOP/s", "frac": tflops / pk, "peak_source": src,
+                    "traffic": None, "flops_per_launch": fpl * links, "avg_launch_ms": f32["kernel_ms"],
+                    "complex_tflops": 8 * nc ** 3 * tensor_products_per_link(len(dims), cfg["level"]) * links
+                    / sec / 1e12}
+    else:
+        roofline = {"bound": "hbm", "kernel": "fused kick+drift (small::k_force<3,float,1>)",
+                    "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                    "peak_source": peak_kind, "traffic": traffic,
+                    "bytes_per_launch": bytes_per_lu * links, "avg_launch_ms": f32["kernel_ms"]}
+    field_mb = links * nc * nc * 8 / 1e6
     line = {
-        "metric": "link-updates/s (1 B200): FP32-mixed HMC trajectories, SU(3) 32^4",
+        "metric": f"link-updates/s (1 B200): FP32-mixed HMC trajectories, SU({nc}) {'x'.join(map(str, dims))}",
         "value": f32["lu"],
         "unit": "link-updates/s",
         "n_gpus": world,
@@ -262,7 +309,8 @@ def run_ours(args):
                                f"BETA={cfg['beta']}, DT={cfg['dt']}, LEVEL={cfg['level']}, "
                                f"{nsteps} MD steps/trajectory, 1 step = 1 trajectory",
                    "links": links, "md_steps_per_traj": nsteps, "parallelism": f"replicas x{world}",
-                   "l2": "inputs larger than L2 (links 302 MB FP32 / 604 MB FP64)"},
+                   "l2": f"links {field_mb:.0f} MB FP32 / {2 * field_mb:.0f} MB FP64 per field; "
+                         f"{'inputs larger than L2' if 2 * field_mb > 126 else 'fields partly L2-resident'}"},
         "trajectories_per_s": world * f32["K"] / (f32["ms"] / 1e3),
         "fp64": {"value": f64["lu"], "ms_per_step": f64["ms"] / f64["K"], "steps": f64["K"],
                  "acceptance": f64["acc"], "mean_abs_dH": f64["dh_abs"]},
@@ -273,10 +321,7 @@ def run_ours(args):
         "plaquette": f32["plaq"],
         "e2e": {"value": f32["e2e_lu"], "unit": "link-updates/s", "h2d_bytes_per_step": f32["h2d"],
                 "d2h_bytes_per_step": f32["d2h"]},
-        "roofline": {"bound": "hbm", "kernel": "fused kick+drift (small::k_force<3,float,1>)",
-                     "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "peak_source": peak_kind, "traffic": traffic,
-                     "bytes_per_launch": bytes_per_lu * links, "avg_launch_ms": f32["kernel_ms"]},
+        "roofline": roofline,
         "gpu_launches": f32["K"] * (nsteps + 15) + f64["K"] * (nsteps + 15),
         "clocks": f32["clocks"],
     }
@@ -344,7 +389,7 @@ def cpu_baseline(cfg, md_steps):
 
 def run_reference_sample(cfg, steps, warmup):
     from oracle import Reference, Oracle, fields
-    nc, dims = cfg["nc"], cfg["dims"]
+    nc, dims = cfg["nc"], cfg.get("cpu_dims", cfg["dims"])
     cores = os.cpu_count() or 1
     rng = np.random.default_rng(1)
     vol = int(np.prod(dims))

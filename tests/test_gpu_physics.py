@@ -110,9 +110,10 @@ def test_fp32_reunitarised_trajectories_stay_unitary():
         assert e.UViol() / (e.vol * e.dim) < 1e-12
 
 
-@pytest.mark.parametrize("nc", [3, 8])
+@pytest.mark.parametrize("nc", [3, 8, 16, 32])
 def test_momentum_refresh_matches_oracle(nc):
-    dims, beta, seed = [4, 3, 2, 2], 4.5, 31337
+    """Thread-per-link refresh (NC < 16) and CTA-per-link refresh (NC >= 16)."""
+    dims, beta, seed = ([4, 3, 2, 2] if nc < 32 else [2, 3, 2]), 4.5, 31337
     O = Oracle(nc, dims)
     with ab.Engine(nc, dims, beta=beta) as e:
         e.initializeE(seed, 5)

@@ -102,6 +102,29 @@ def test_matches_cuda_core_fp32_trajectory():
     assert res[2]["h_old"] == pytest.approx(res[0]["h_old"], rel=1e-6)
 
 
+@pytest.mark.parametrize("nc,dims,precision", [(16, [2, 3, 2], "fp64"), (32, [2, 2, 3], "fp64"),
+                                               (64, [2, 3], "fp64"), (32, [2, 2, 3], "fp32")])
+def test_large_nc_reductions_vs_oracle(nc, dims, precision):
+    """CTA-per-site plaquette sums and CTA-per-link kinetic / UViol sums
+    (NC >= 16), accumulated in FP64 for either storage precision."""
+    O, u, pi, beta = setup(nc, dims, 5 * nc)
+    Pi = fields.momenta(nc, O.vol * O.dim, beta, np.random.default_rng(nc + 1), O)
+    if precision == "fp32":  # compare on the FP32-rounded inputs the engine actually holds
+        u = u.astype(np.complex64).astype(np.complex128)
+        pi = pi.astype(np.complex64).astype(np.complex128)
+        Pi = Pi.astype(np.complex64).astype(np.complex128)
+    with ab.Engine(nc, dims, beta=beta, precision=precision) as e:
+        e.set_links(u)
+        e.set_momenta(pi, 0)
+        e.set_momenta(Pi, 1)
+        assert e.EnergyMag() == pytest.approx(O.EnergyMag(u), rel=1e-12)
+        t, s = e.PlaqExp()
+        assert t + s == pytest.approx(O.EnergyMag(u), rel=1e-12)
+        assert e.simpleenergyEl(0) == pytest.approx(O.simpleenergyEl(pi), rel=1e-12)
+        assert e.EnergyEl() == pytest.approx(O.EnergyEl(pi, Pi), rel=1e-12)
+        assert e.UViol() == pytest.approx(O.UViol(u), rel=1e-6, abs=1e-18 * O.vol * O.dim)
+
+
 def test_path_validation():
     with pytest.raises(ab.AskjaError):
         ab.Engine(32, [2, 2], beta=1.0, precision="fp64", kernel_path=2)
