@@ -8,7 +8,9 @@
 //           (sun.cpp:702-716, Adjoint = sunmat.h:355-371)
 //   kick    P <- P - eps * F
 //   drift   U <- exp(i eps P) U, Taylor order `order` in Horner form
-//           (sunmat.h:200-248, applied to U directly: U + X(U + X/2(U + ...)))
+//           (sunmat.h:200-248, applied to U directly: U + X(U + X/2(U + ...)));
+//           the FP32 path sums the same series through Cayley-Hamilton
+//           (two matrix products instead of `order`, expi_times_ch)
 // with the staple product factored as U_mu(x) * (sum of the remaining three
 // links), which saves one matrix product per staple against the reference's
 // left-to-right evaluation; results agree to rounding.
@@ -191,6 +193,128 @@ __device__ __forceinline__ void expi_times(Mat<N, T>& Tm, const Mat<N, T>& P, co
   }
 }
 
+template <typename T>
+__device__ __forceinline__ cpx<T> cmul(const cpx<T>& a, const cpx<T>& b) {
+  cpx<T> z = czero<T>();
+  cmac(z, a, b);
+  return z;
+}
+
+// The same truncated series sum_{k<=order} X^k / k!, X = i eps P, for N = 2
+// and 3, evaluated through the Cayley-Hamilton theorem instead of Horner:
+// X^N is a combination of 1 .. X^(N-1) (coefficients from tr X, tr X^2 and
+// det X), so X^k = al_k 1 + be_k X (+ ga_k X^2) with a scalar recursion, and
+// E = sum (al_k, be_k, ga_k) / k! needs one matrix product (X^2, N = 3) before
+// the final E U -- two products instead of `order`.  Exact in real
+// arithmetic for any X (no hermiticity assumed); rounding differs from
+// Horner at the level of the storage precision.
+template <int N, typename T>
+__device__ __forceinline__ void expi_times_ch(Mat<N, T>& Tm, const Mat<N, T>& P, const Mat<N, T>& Ux, T eps,
+                                              int order) {
+  static_assert(N == 2 || N == 3, "Cayley-Hamilton form for N = 2, 3");
+  Mat<N, T> X;
+#pragma unroll
+  for (int i = 0; i < N; i++)
+#pragma unroll
+    for (int j = 0; j < N; j++) X.a[i][j] = mkc<T>(-eps * P.a[i][j].im, eps * P.a[i][j].re);
+  cpx<T> tr = czero<T>();
+#pragma unroll
+  for (int i = 0; i < N; i++) {
+    tr.re += X.a[i][i].re;
+    tr.im += X.a[i][i].im;
+  }
+  Mat<N, T> E;
+  if constexpr (N == 2) {
+    // X^2 = tr X X - det X 1
+    cpx<T> d = cmul(X.a[0][0], X.a[1][1]);
+    cmsub(d, X.a[0][1], X.a[1][0]);
+    cpx<T> al = mkc<T>(T(1), T(0)), be = czero<T>();  // X^0
+    cpx<T> sa = al, sb = be;
+    T f = T(1);
+    for (int k = 1; k <= order; k++) {
+      // X^k = -be_{k-1} det 1 + (al_{k-1} + be_{k-1} tr) X
+      cpx<T> nal = czero<T>(), nbe = al;
+      cmsub(nal, be, d);
+      cmac(nbe, be, tr);
+      al = nal;
+      be = nbe;
+      f = f / T(k);
+      sa.re = fma(f, al.re, sa.re);
+      sa.im = fma(f, al.im, sa.im);
+      sb.re = fma(f, be.re, sb.re);
+      sb.im = fma(f, be.im, sb.im);
+    }
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+      for (int j = 0; j < 2; j++) {
+        cpx<T> e = i == j ? sa : czero<T>();
+        cmac(e, sb, X.a[i][j]);
+        E.a[i][j] = e;
+      }
+  } else {
+    Mat<N, T> X2;
+    mul_nn(X2, X, X);
+    cpx<T> tr2 = czero<T>();
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+      tr2.re += X2.a[i][i].re;
+      tr2.im += X2.a[i][i].im;
+    }
+    // c1 = ((tr X)^2 - tr X^2) / 2, c0 = det X; X^3 = tr X X^2 - c1 X + c0 1
+    cpx<T> c1 = cmul(tr, tr);
+    c1.re = T(0.5) * (c1.re - tr2.re);
+    c1.im = T(0.5) * (c1.im - tr2.im);
+    cpx<T> m0 = cmul(X.a[1][1], X.a[2][2]), m1 = cmul(X.a[1][0], X.a[2][2]), m2 = cmul(X.a[1][0], X.a[2][1]);
+    cmsub(m0, X.a[1][2], X.a[2][1]);
+    cmsub(m1, X.a[1][2], X.a[2][0]);
+    cmsub(m2, X.a[1][1], X.a[2][0]);
+    cpx<T> c0 = cmul(X.a[0][0], m0);
+    cmsub(c0, X.a[0][1], m1);
+    cmac(c0, X.a[0][2], m2);
+    cpx<T> al = mkc<T>(T(1), T(0)), be = czero<T>(), ga = czero<T>();  // X^0
+    cpx<T> sa = al, sb = be, sc = ga;
+    T f = T(1);
+    for (int k = 1; k <= order; k++) {
+      // X^k = ga c0 1 + (al - ga c1) X + (be + ga tr) X^2  (coefficients of X^(k-1))
+      const cpx<T> nal = cmul(ga, c0);
+      cpx<T> nbe = al, nga = be;
+      cmsub(nbe, ga, c1);
+      cmac(nga, ga, tr);
+      al = nal;
+      be = nbe;
+      ga = nga;
+      f = f / T(k);
+      sa.re = fma(f, al.re, sa.re);
+      sa.im = fma(f, al.im, sa.im);
+      sb.re = fma(f, be.re, sb.re);
+      sb.im = fma(f, be.im, sb.im);
+      sc.re = fma(f, ga.re, sc.re);
+      sc.im = fma(f, ga.im, sc.im);
+    }
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+      for (int j = 0; j < 3; j++) {
+        cpx<T> e = i == j ? sa : czero<T>();
+        cmac(e, sb, X.a[i][j]);
+        cmac(e, sc, X2.a[i][j]);
+        E.a[i][j] = e;
+      }
+  }
+  mul_nn(Tm, E, Ux);
+}
+
+// Link update of the FP32 path: the Cayley-Hamilton form where it exists;
+// the FP64 path keeps the reference's Horner evaluation.
+template <int N, typename T>
+__device__ __forceinline__ void expi_update(Mat<N, T>& Tm, const Mat<N, T>& P, const Mat<N, T>& Ux, T eps, int order) {
+  if constexpr (sizeof(T) == 4 && N <= 3)
+    expi_times_ch(Tm, P, Ux, eps, order);
+  else
+    expi_times(Tm, P, Ux, eps, order);
+}
+
 // Project onto SU(N): modified Gram-Schmidt of rows 0..N-2 (in order), then
 // the last row is the unique unit row that completes them to determinant 1
 // (the conjugated generalised cross product of the other rows).
@@ -280,7 +404,7 @@ __device__ __forceinline__ void force_link(const Lat& L, const S2* __restrict__ 
   store(Pout, P, L, mu, x);
   if (MODE == 1) {
     Mat<N, T> Tm;
-    expi_times(Tm, P, Ux, eps_d, order);
+    expi_update(Tm, P, Ux, eps_d, order);
     if (reunit) reunitarise(Tm);
     store(Uout, Tm, L, mu, x);
   }
@@ -320,7 +444,7 @@ __global__ void __launch_bounds__(128) k_drift(Lat L, S2* __restrict__ U, const 
   Mat<N, T> Ux, Pm, Tm;
   load(Ux, U, L, mu, x);
   load(Pm, P, L, mu, x);
-  expi_times(Tm, Pm, Ux, eps, order);
+  expi_update(Tm, Pm, Ux, eps, order);
   if (reunit) reunitarise(Tm);
   store(U, Tm, L, mu, x);
 }
