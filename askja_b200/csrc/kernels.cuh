@@ -135,9 +135,26 @@ cudaError_t tc_link(const LaunchCtx& c, int mode, const void* U, const void* Pin
   auto k = mode == 0 ? tc::k_link<NC, 0> : mode == 1 ? tc::k_link<NC, 1> : tc::k_link<NC, 2>;
   const size_t smem = tc::Shape<NC>::SMEM;
   if ((e = set_smem(k, smem)) != cudaSuccess) return e;
-  int per = 0;
-  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, tc::THREADS, smem)) != cudaSuccess) return e;
-  const long grid = std::min(nlinks(L), (long)nsm * std::max(per, 1));
+  // the whole unified L1/shared array as shared memory, so that as many CTAs
+  // as registers and shared memory allow are resident (TMEM: 4 NC columns
+  // each; shared memory admits at most 4 CTAs of NC = 32 and 1 of NC = 64,
+  // so the allocations never exceed the 512 columns of an SM)
+  if ((e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                (int)cudaSharedmemCarveoutMaxShared)) != cudaSuccess)
+    return e;
+  // resident CTAs per SM from registers, shared memory, threads and tensor
+  // memory (the occupancy query reports 1 for these kernels)
+  cudaFuncAttributes fa{};
+  if ((e = cudaFuncGetAttributes(&fa, k)) != cudaSuccess) return e;
+  int smem_sm = 0, smem_rsv = 0, regs_sm = 0;
+  if ((e = cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev)) != cudaSuccess) return e;
+  if ((e = cudaDeviceGetAttribute(&smem_rsv, cudaDevAttrReservedSharedMemoryPerBlock, dev)) != cudaSuccess) return e;
+  if ((e = cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev)) != cudaSuccess) return e;
+  const int regs = (std::max(fa.numRegs, 1) + 7) / 8 * 8;
+  int per = std::min(regs_sm / (regs * tc::THREADS), smem_sm / (int)(smem + fa.sharedSizeBytes + smem_rsv));
+  per = std::min(per, 2048 / tc::THREADS);
+  per = std::max(1, std::min(per, 512 / tc::Shape<NC>::TMEM_COLS));
+  const long grid = std::min(nlinks(L), (long)nsm * per);
   k<<<(unsigned)grid, tc::THREADS, smem, c.stream>>>(L, aos, static_cast<const float2*>(Pin),
                                                       static_cast<float2*>(Pout), static_cast<float2*>(Uout),
                                                       (float)ek, (float)ed, c.order, c.reunit, c.status);

@@ -545,6 +545,35 @@ def run_reference(args):
     return line
 
 
+def run_kernel_only(args):
+    """Kernel microbenchmark (also the command the ncu summaries under
+    profiles/ capture): one engine of the config, Haar hot start, Philox
+    momenta, then `--steps` fused kick+drift launches (askja_leapfrog: steps
+    fused launches + 1 kick) with the default (untuned) kernel mapping or the
+    one `--path` forces.  Prints the average launch time."""
+    import torch
+
+    import askja_b200 as ab
+    cfg = CONFIGS[args.config]
+    nc, dims = cfg["nc"], cfg["dims"]
+    with ab.Engine(nc, dims, beta=cfg["beta"], dt=cfg["dt"], level=cfg["level"], precision=args.precision,
+                   kernel_path=args.path) as e:
+        e.hot_start(11)
+        e.initializeE(11, 0)
+        for _ in range(args.warmup):
+            e.leapfrog(1, cfg["dt"])
+        e.sync()
+        s, t0, t1 = event_timer(e.stream_ptr, 0)
+        t0.record(s)
+        e.leapfrog(args.steps, cfg["dt"])
+        t1.record(s)
+        t1.synchronize()
+        ms = t0.elapsed_time(t1) / (args.steps + 1)
+    return {"kernel_only": args.config, "precision": args.precision, "path": args.path,
+            "launches": args.steps + 1, "avg_launch_ms": ms,
+            "link_updates_per_s": int(np.prod(dims)) * len(dims) / (ms / 1e3)}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -555,8 +584,13 @@ def main():
     ap.add_argument("--cpu-md-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-precision", action="store_true")
+    ap.add_argument("--kernel-only", action="store_true", help="fused-kernel microbenchmark (profiling)")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"], help="with --kernel-only")
+    ap.add_argument("--path", type=int, default=0, help="with --kernel-only: askja kernel_path")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.kernel_only:
+        line = run_kernel_only(args)
+    elif args.impl == "reference":
         line = run_reference(args)
     elif args.config == "batch64":
         line = run_batch(args)
