@@ -150,7 +150,10 @@ __device__ __forceinline__ void kick_ta(Mat<N, T>& P, const Mat<N, T>& W, T eps)
   T trim = T(0);
 #pragma unroll
   for (int k = 0; k < N; k++) trim += W.a[k][k].im;
-  trim = trim / T(N);
+  if constexpr (sizeof(T) == 4)
+    trim = trim * (T(1) / T(N));  // FP32: a constant multiply instead of a division
+  else
+    trim = trim / T(N);
 #pragma unroll
   for (int i = 0; i < N; i++)
 #pragma unroll
@@ -231,14 +234,16 @@ __device__ __forceinline__ void expi_times_ch(Mat<N, T>& Tm, const Mat<N, T>& P,
     cpx<T> al = mkc<T>(T(1), T(0)), be = czero<T>();  // X^0
     cpx<T> sa = al, sb = be;
     T f = T(1);
-    for (int k = 1; k <= order; k++) {
+#pragma unroll
+    for (int k = 1; k <= 8; k++) {  // order <= 8; unrolled so that 1/k is a constant
+      if (k > order) break;
       // X^k = -be_{k-1} det 1 + (al_{k-1} + be_{k-1} tr) X
       cpx<T> nal = czero<T>(), nbe = al;
       cmsub(nal, be, d);
       cmac(nbe, be, tr);
       al = nal;
       be = nbe;
-      f = f / T(k);
+      f = f * T(1.0 / k);
       sa.re = fma(f, al.re, sa.re);
       sa.im = fma(f, al.im, sa.im);
       sb.re = fma(f, be.re, sb.re);
@@ -275,7 +280,9 @@ __device__ __forceinline__ void expi_times_ch(Mat<N, T>& Tm, const Mat<N, T>& P,
     cpx<T> al = mkc<T>(T(1), T(0)), be = czero<T>(), ga = czero<T>();  // X^0
     cpx<T> sa = al, sb = be, sc = ga;
     T f = T(1);
-    for (int k = 1; k <= order; k++) {
+#pragma unroll
+    for (int k = 1; k <= 8; k++) {  // order <= 8; unrolled so that 1/k is a constant
+      if (k > order) break;
       // X^k = ga c0 1 + (al - ga c1) X + (be + ga tr) X^2  (coefficients of X^(k-1))
       const cpx<T> nal = cmul(ga, c0);
       cpx<T> nbe = al, nga = be;
@@ -284,7 +291,7 @@ __device__ __forceinline__ void expi_times_ch(Mat<N, T>& Tm, const Mat<N, T>& P,
       al = nal;
       be = nbe;
       ga = nga;
-      f = f / T(k);
+      f = f * T(1.0 / k);
       sa.re = fma(f, al.re, sa.re);
       sa.im = fma(f, al.im, sa.im);
       sb.re = fma(f, be.re, sb.re);

@@ -250,7 +250,10 @@ def run_ours(args):
                        seed=seed) as e:
             e.hot_start(seed + 1)
             e.initializeE(seed, 0)
-            tuning = ab.autotune(e, reps=3)  # untimed: picks the kernel mapping for this (NC, DIM, precision)
+            # untimed: picks the kernel mapping for this (NC, DIM, precision); --no-tune keeps the
+            # default mapping (under a profiler the candidates' timings are not representative)
+            tuning = {"path": None, "groups": 0, "occupancy": 0, "best_us": None} if args.no_tune \
+                else ab.autotune(e, reps=3)
             K = args.steps if prec == "fp32" else max(3, args.steps // 2)
             clocks = Clocks(dev) if prec == "fp32" else None
             ms, last, log = time_trajectories(e, e.stream_ptr, dev, nsteps, K, args.warmup, world, clocks)
@@ -585,6 +588,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-precision", action="store_true")
     ap.add_argument("--kernel-only", action="store_true", help="fused-kernel microbenchmark (profiling)")
+    ap.add_argument("--no-tune", action="store_true", help="default kernel mapping, no autotuning")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"], help="with --kernel-only")
     ap.add_argument("--path", type=int, default=0, help="with --kernel-only: askja kernel_path")
     args = ap.parse_args()
