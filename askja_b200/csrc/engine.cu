@@ -135,10 +135,24 @@ int launch_ok(askja_ctx* c, cudaError_t e, const char* what) {
     if (rc_) return rc_;                          \
   } while (0)
 
+// tensor-core path: trajectories between two Gram-Schmidt passes over U
+constexpr int TC_REUNIT_EVERY = 10;
+
 // Enqueue one whole trajectory (no host synchronisation; graph-capturable).
 int enqueue_trajectory(askja_ctx* c, int nsteps) {
   const double dt = c->p.dt;
   const double scale = std::sqrt(2.0 * c->N / c->p.beta);
+  if (c->lc.force_rows == 2 && c->lc.reunit) {
+    // the tensor-core link update keeps U' exactly as unitary as U (it
+    // projects exp(i eps P), not U'); the rounding defect U accumulates (an
+    // unbiased random walk, ~6e-8 sqrt(MD steps)) is removed here, before
+    // every TC_REUNIT_EVERY-th trajectory, and the saved copy follows
+    askja::LaunchCtx lc = c->lc;
+    lc.gate = &c->st->traj;
+    lc.gate_every = TC_REUNIT_EVERY;
+    KL(c->ks->reunit(lc, cur_u(c)), "reunitarise");
+    KL(cudaMemcpyAsync(c->Uconf, cur_u(c), c->field_bytes, cudaMemcpyDeviceToDevice, c->stream), "save links");
+  }
   KL(c->ks->refresh(c->lc, c->P, c->p.seed, &c->st->traj, 0, scale), "refresh");
   KL(c->ks->plaq(c->lc, cur_u(c), c->partial, c->sums), "plaq");
   KL(c->ks->linksums(c->lc, c->P, nullptr, nullptr, c->partial, c->sums + 2), "kinetic");

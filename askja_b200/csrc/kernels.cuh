@@ -231,7 +231,7 @@ cudaError_t reunit(const LaunchCtx& c, void* U) {
   auto k = rows::k_reunit<T, S2>;
   cudaError_t e;
   if ((e = set_smem(k, smem)) != cudaSuccess) return e;
-  k<<<blocks_for(nlinks(c.lat), G), G * N, smem, c.stream>>>(c.lat, (S2*)U);
+  k<<<blocks_for(nlinks(c.lat), G), G * N, smem, c.stream>>>(c.lat, (S2*)U, c.gate, c.gate_every);
   return cudaGetLastError();
 }
 

@@ -21,6 +21,9 @@ struct LaunchCtx {
   int small_occ;    // thread-per-link kernels: 1 = higher-occupancy register budget
   void* scratch;    // tensor-core path: per-link contiguous copy of U (V*D*NC*NC float2)
   unsigned* status; // tensor-core path: nonzero after a bounded wait gave up
+  // row-kernel reunitarisation: run only when *gate % gate_every == 0 (null: always)
+  const unsigned long long* gate;
+  int gate_every;
 };
 
 // whether the tensor-core mapping exists for this shape and precision

@@ -506,8 +506,12 @@ __global__ void k_drift(Lat L, S2* __restrict__ U, const S2* __restrict__ P, T e
 }
 
 // In-place reunitarisation of every link (also used for the Haar hot start).
+// With a gate, the launch does nothing unless *gate % every == 0 (a counter
+// in device memory, so that a captured trajectory graph can run it on every
+// `every`-th replay).
 template <typename T, typename S2>
-__global__ void k_reunit(Lat L, S2* __restrict__ U) {
+__global__ void k_reunit(Lat L, S2* __restrict__ U, const unsigned long long* __restrict__ gate, int every) {
+  if (gate && every > 1 && (*gate % (unsigned long long)every) != 0) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int piv_s[64];
   __shared__ cpx<T> det_s[64];

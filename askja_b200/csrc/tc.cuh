@@ -39,11 +39,13 @@
 // a per-link contiguous copy of U (k_to_aos), P and the outputs use the
 // blocked field layout of common.cuh.
 //
-// Reunitarisation after the link update is one Newton-Schulz polar step
-// U <- U (3 - U^dag U) / 2 on the tensor cores (unitarity back to FP32
-// rounding; the determinant phase is not re-fixed here: exp(i eps P) of a
-// traceless P has determinant 1 up to the Taylor remainder, so the phase only
-// drifts by rounding; askja_reunitarise fixes it on demand).
+// The link update is carried as U' = U + (E - 1) U with E = exp(i eps P) to
+// order LEVEL, so the tensor cores only form products of small matrices and
+// the O(1) parts are added in FP32 on the CUDA cores.  Reunitarisation projects
+// E onto the unitary group by one Newton-Schulz step E (3 - E^dag E)/2,
+// itself formed from small products, so U' is as unitary as U; U's own
+// rounding defect (an unbiased random walk) is removed between trajectories
+// by the CUDA-core Gram-Schmidt kernel (the engine does this for this path).
 #pragma once
 
 #include "common.cuh"
@@ -363,68 +365,48 @@ struct Role {
     }
     im = rr >= NC;
     m = im ? rr - NC : rr;
+    if (!valid) {  // lanes 16..31 of each warp when M = 64: no accumulator row
+      im = false;
+      m = 0;
+    }
     lane = (uint32_t)(32 * q) << 16;
   }
 };
 
-// left operand from the accumulator row: X = D (scale 1) or, for the Horner
-// step, X = 1 + (i sc) D
+// left operand, one row part of one plane: x = row m, columns c0.. of the
+// real (imag = false) or imaginary part of X
 template <int NC>
-__device__ __forceinline__ void epi_A(const Smem& s, const Role<NC>& ro, const float* v, bool horner, float sc) {
+__device__ __forceinline__ void put_row_A(const Smem& s, const Role<NC>& ro, const float* x, bool imag) {
   if (!ro.valid) return;
 #pragma unroll
   for (int q = 0; q < Shape<NC>::HALF / 4; q++) {
     const int k0 = ro.c0 + 4 * q;
-    float4 x = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
-    if (!horner) {
-      if (!ro.im) {
-        st4<NC>(s.A, Shape<NC>::A_BYTES, opoff<NC>(NC + ro.m, k0), x);
-      } else {
-        st4<NC>(s.A, Shape<NC>::A_BYTES, opoff<NC>(2 * NC + ro.m, k0), x);
-        st4<NC>(s.A, Shape<NC>::A_BYTES, opoff<NC>(ro.m, k0), neg4(x));
-      }
-    } else if (!ro.im) {  // Xi = sc Dr
-      const float4 y = make_float4(sc * x.x, sc * x.y, sc * x.z, sc * x.w);
+    const float4 y = make_float4(x[4 * q], x[4 * q + 1], x[4 * q + 2], x[4 * q + 3]);
+    if (!imag) {
+      st4<NC>(s.A, Shape<NC>::A_BYTES, opoff<NC>(NC + ro.m, k0), y);
+    } else {
       st4<NC>(s.A, Shape<NC>::A_BYTES, opoff<NC>(2 * NC + ro.m, k0), y);
       st4<NC>(s.A, Shape<NC>::A_BYTES, opoff<NC>(ro.m, k0), neg4(y));
-    } else {  // Xr = 1 - sc Di
-      float4 y = make_float4(-sc * x.x, -sc * x.y, -sc * x.z, -sc * x.w);
-      if (ro.m == k0) y.x += 1.f;
-      if (ro.m == k0 + 1) y.y += 1.f;
-      if (ro.m == k0 + 2) y.z += 1.f;
-      if (ro.m == k0 + 3) y.w += 1.f;
-      st4<NC>(s.A, Shape<NC>::A_BYTES, opoff<NC>(NC + ro.m, k0), y);
     }
   }
 }
 
-// left operand X = D^dag from the accumulator row (transposed stores)
+// left operand X = D from the accumulator row
 template <int NC>
-__device__ __forceinline__ void epi_A_dag(const Smem& s, const Role<NC>& ro, const float* v) {
-  if (!ro.valid) return;
-#pragma unroll
-  for (int c = 0; c < Shape<NC>::HALF; c++) {
-    const int j = ro.c0 + c;  // D[m][j] -> X[j][m]
-    if (!ro.im) {
-      st1<NC>(s.A, Shape<NC>::A_BYTES, opoff<NC>(NC + j, ro.m), v[c]);
-    } else {
-      st1<NC>(s.A, Shape<NC>::A_BYTES, opoff<NC>(2 * NC + j, ro.m), -v[c]);
-      st1<NC>(s.A, Shape<NC>::A_BYTES, opoff<NC>(j, ro.m), v[c]);
-    }
-  }
+__device__ __forceinline__ void epi_A(const Smem& s, const Role<NC>& ro, const float* v) {
+  put_row_A<NC>(s, ro, v, ro.im);
 }
 
-// right operand B = D (zmap = false) or B = 3/2 - D/2 (zmap = true) from the
-// accumulator row: Bs[j][m] = D[m][j] (transposed stores)
+// right operand B = D from the accumulator row: Bs[j][m] = D[m][j]
+// (transposed stores)
 template <int NC>
-__device__ __forceinline__ void epi_B(const Smem& s, const Role<NC>& ro, const float* v, bool zmap) {
+__device__ __forceinline__ void epi_B(const Smem& s, const Role<NC>& ro, const float* v) {
   if (!ro.valid) return;
   unsigned char* base = s.B + (ro.im ? 2 * Shape<NC>::B_BYTES : 0);
 #pragma unroll
   for (int c = 0; c < Shape<NC>::HALF; c++) {
     const int j = ro.c0 + c;
-    float x = v[c];
-    if (zmap) x = (!ro.im && j == ro.m ? 1.5f : 0.f) - 0.5f * x;
+    const float x = v[c];
     st1<NC>(base, Shape<NC>::B_BYTES, opoff<NC>(j, ro.m), x);
   }
 }
@@ -561,7 +543,7 @@ __global__ void __launch_bounds__(THREADS, NC == 64 ? 1 : 3)
         ok = done(s, phase);
         if (!ok) break;
         acc_row<NC>(tT + ro.lane + ro.c0, v);
-        epi_A<NC>(s, ro, v, false, 0.f);
+        epi_A<NC>(s, ro, v);
         put<NC>(s, fb1, t.kb2);
         go<NC>(s, tS, i > 0 ? 1u : 0u);
         if (i + 1 < nterms) {
@@ -576,7 +558,7 @@ __global__ void __launch_bounds__(THREADS, NC == 64 ? 1 : 3)
       if (!ok) break;
       // ---- W = U_mu(x) S  (TMEM columns 0..NC-1)
       acc_row<NC>(tS + ro.lane + ro.c0, v);
-      epi_B<NC>(s, ro, v, false);
+      epi_B<NC>(s, ro, v);
       put<NC>(s, fa, A_NORM);
       go<NC>(s, tT, 0);
       float2 pn[SH::EPT];
@@ -626,24 +608,32 @@ __global__ void __launch_bounds__(THREADS, NC == 64 ? 1 : 3)
       }
       __syncthreads();
     }
-    // ---- drift: E = 1 + (i eps/L) P, E <- 1 + (i eps/k) E P (k = L-1..1), U' = E U
+    // ---- drift with E = 1 + Em, so that the tensor cores only form small
+    // products (their accumulation of O(1) sums is biased at ~1e-6 per
+    // product, which a per-step projection would turn into an energy drift):
+    //   Em = (i eps/L) P;  Em <- (i eps/k) (P + Em P),  k = L-1..1
+    //   reunit: Ep = E (3 - E^dag E)/2 - 1 = Em - (M + Em M)/2,
+    //           M = Em + Em^dag + Em^dag Em    (Newton-Schulz on E, not on U')
+    //   U' = U + Ep U
+    // The O(1) terms (P, U, the diagonal of E) enter by FP32 additions on the
+    // CUDA cores.  U's own unitarity defect is corrected between trajectories.
     {
+      const int src = ro.im ? NC : 0;  // plane of this thread's accumulator row
+      const int dst = ro.im ? 0 : NC;  // plane of Em this row produces (i times it)
       const float sc0 = order > 0 ? eps_d / (float)order : 0.f;
+      float em[SH::HALF];
 #pragma unroll
-      for (int i = 0; i < SH::UPT; i++) {
+      for (int i = 0; i < SH::UPT; i++) {  // A <- Em = i sc0 P
         int m, kc;
         unit_rc<NC>(tid + THREADS * i, true, m, kc);
         const float* rp = s.plain + m * SH::PS + 4 * kc;
         const float* ip = s.plain + (NC + m) * SH::PS + 4 * kc;
-        const float4 pr = make_float4(rp[0], rp[1], rp[2], rp[3]);
-        const float4 pi = make_float4(ip[0], ip[1], ip[2], ip[3]);
-        float4 er = make_float4(-sc0 * pi.x, -sc0 * pi.y, -sc0 * pi.z, -sc0 * pi.w);
-        if (m == 4 * kc) er.x += 1.f;
-        if (m == 4 * kc + 1) er.y += 1.f;
-        if (m == 4 * kc + 2) er.z += 1.f;
-        if (m == 4 * kc + 3) er.w += 1.f;
-        put_A<NC>(s, m, kc, er, make_float4(sc0 * pr.x, sc0 * pr.y, sc0 * pr.z, sc0 * pr.w));
+        put_A<NC>(s, m, kc, make_float4(-sc0 * ip[0], -sc0 * ip[1], -sc0 * ip[2], -sc0 * ip[3]),
+                  make_float4(sc0 * rp[0], sc0 * rp[1], sc0 * rp[2], sc0 * rp[3]));
       }
+#pragma unroll
+      for (int c = 0; c < SH::HALF; c++)
+        em[c] = ro.valid ? (ro.im ? -sc0 : sc0) * s.plain[(src + ro.m) * SH::PS + ro.c0 + c] : 0.f;
       if (order > 1) {
 #pragma unroll
         for (int i = 0; i < SH::UPT; i++) {  // B = P: Bs[j][k] = P[k][j]
@@ -660,31 +650,73 @@ __global__ void __launch_bounds__(THREADS, NC == 64 ? 1 : 3)
         go<NC>(s, tT, 0);
         ok = done(s, phase);
         if (!ok) break;
-        acc_row<NC>(tT + ro.lane + ro.c0, v);
-        epi_A<NC>(s, ro, v, true, eps_d / (float)k);
+        acc_row<NC>(tT + ro.lane + ro.c0, v);  // (Em P) row
+        const float sc = (ro.im ? -eps_d : eps_d) / (float)k;
+#pragma unroll
+        for (int c = 0; c < SH::HALF; c++)
+          em[c] = ro.valid ? sc * (v[c] + s.plain[(src + ro.m) * SH::PS + ro.c0 + c]) : 0.f;
+        put_row_A<NC>(s, ro, em, !ro.im);
       }
       if (!ok) break;
+      __syncthreads();  // every read of P is done: the plain tile now takes Em
+      if (ro.valid)
+#pragma unroll
+        for (int c = 0; c < SH::HALF; c++) s.plain[(dst + ro.m) * SH::PS + ro.c0 + c] = em[c];
+      __syncthreads();
+      if (reunit) {
+#pragma unroll
+        for (int i = 0; i < SH::UPT; i++) {  // A <- Em^dag, B <- Em, from columns of the plain tile
+          int r, kc;
+          unit_rc<NC>(tid + THREADS * i, false, r, kc);
+          const float* pr = s.plain + 4 * kc * SH::PS + r;
+          const float* pi = s.plain + (NC + 4 * kc) * SH::PS + r;
+          const float4 re = make_float4(pr[0], pr[SH::PS], pr[2 * SH::PS], pr[3 * SH::PS]);
+          const float4 im = make_float4(pi[0], pi[SH::PS], pi[2 * SH::PS], pi[3 * SH::PS]);
+          put_A<NC>(s, r, kc, re, neg4(im));
+          put_B<NC>(s, r, kc, re, im);
+        }
+        go<NC>(s, tS, 0);
+        ok = done(s, phase);
+        if (!ok) break;
+        acc_row<NC>(tS + ro.lane + ro.c0, v);  // (Em^dag Em) row
+        float mm[SH::HALF];
+#pragma unroll
+        for (int c = 0; c < SH::HALF; c++) {
+          const int j = ro.c0 + c;
+          const float t = s.plain[(src + j) * SH::PS + ro.m];
+          mm[c] = ro.valid ? s.plain[(src + ro.m) * SH::PS + j] + (ro.im ? -t : t) + v[c] : 0.f;
+        }
+        epi_B<NC>(s, ro, mm);  // B <- M
+#pragma unroll
+        for (int i = 0; i < SH::UPT; i++) {  // A <- Em
+          int m, kc;
+          unit_rc<NC>(tid + THREADS * i, true, m, kc);
+          const float* rp = s.plain + m * SH::PS + 4 * kc;
+          const float* ip = s.plain + (NC + m) * SH::PS + 4 * kc;
+          put_A<NC>(s, m, kc, make_float4(rp[0], rp[1], rp[2], rp[3]), make_float4(ip[0], ip[1], ip[2], ip[3]));
+        }
+        go<NC>(s, tT, 0);
+        ok = done(s, phase);
+        if (!ok) break;
+        acc_row<NC>(tT + ro.lane + ro.c0, v);  // (Em M) row
+#pragma unroll
+        for (int c = 0; c < SH::HALF; c++)
+          em[c] = ro.valid ? s.plain[(src + ro.m) * SH::PS + ro.c0 + c] - 0.5f * (mm[c] + v[c]) : 0.f;
+        put_row_A<NC>(s, ro, em, ro.im);  // A <- Ep
+      }
       put<NC>(s, fa, B_NORM);
       go<NC>(s, tT, 0);
       ok = done(s, phase);
       if (!ok) break;
-      acc_row<NC>(tT + ro.lane + ro.c0, v);
-    }
-    if (reunit) {
-      // Newton-Schulz polar step: Y = U'^dag U', U'' = U' (3 - Y)/2
-      epi_A_dag<NC>(s, ro, v);
-      epi_B<NC>(s, ro, v, false);
-      go<NC>(s, tS, 0);
-      ok = done(s, phase);
-      if (!ok) break;
-      float y[SH::HALF];
-      acc_row<NC>(tS + ro.lane + ro.c0, y);
-      epi_B<NC>(s, ro, y, true);
-      epi_A<NC>(s, ro, v, false, 0.f);
-      go<NC>(s, tT, 0);
-      ok = done(s, phase);
-      if (!ok) break;
-      acc_row<NC>(tT + ro.lane + ro.c0, v);
+      acc_row<NC>(tT + ro.lane + ro.c0, v);  // (Ep U) row
+      if (ro.valid) {
+        const float2* ur = ulink + ro.m * NC + ro.c0;
+#pragma unroll
+        for (int c = 0; c < SH::HALF; c++) {
+          const float2 u = __ldg(ur + c);
+          v[c] += ro.im ? u.y : u.x;
+        }
+      }
     }
     epi_plain<NC>(s, ro, v);
     __syncthreads();
