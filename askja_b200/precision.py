@@ -95,25 +95,36 @@ def compare(nc, dims, beta, dt, level, nsteps, u0, ntraj_dh=3, seed=7, device=0)
 def ensemble(nc, dims, beta, dt, level, nsteps, u0, ntraj, seed=11, device=0):
     res = {}
     vol = int(np.prod(dims))
-    nplaq = vol * len(dims) * (len(dims) - 1) // 2
+    D = len(dims)
+    nplaq = vol * D * (D - 1) // 2
+    nt, ns = vol * (D - 1), vol * (D - 1) * (D - 2) // 2  # temporal (0,k) / spatial (j,k) planes
+    obs = ("plaquette", "plaquette_t", "plaquette_s", "polyakov", "wilson")
     for prec in ("fp64", "fp32"):
         with Engine(nc, dims, beta=beta, dt=dt, level=level, precision=prec, device=device, seed=seed) as e:
             e.set_links(u0)
-            plaq, poly, acc = [], [], 0
+            series = {k: [] for k in obs}
+            acc = 0
             t0 = time.perf_counter()
             for _ in range(ntraj):
                 last, _ = e.run_trajectories(1, nsteps, use_graph=True, want_log=False)
                 acc += int(last["accepted"] != 0)
-                s = e.EnergyMag()
-                plaq.append(1.0 - s / nplaq)
-                poly.append(e.PolyakovLoop())
-            res[prec] = {"plaquette": float(np.mean(plaq)), "plaquette_err": _binned_error(np.array(plaq)),
-                         "polyakov": float(np.mean(poly)), "polyakov_err": _binned_error(np.array(poly)),
-                         "acceptance": acc / max(1, ntraj), "seconds": time.perf_counter() - t0}
-    d = res["fp32"]["plaquette"] - res["fp64"]["plaquette"]
-    sig = float(np.hypot(res["fp32"]["plaquette_err"], res["fp64"]["plaquette_err"]))
-    res["plaquette_diff"] = d
-    res["plaquette_diff_in_sigma"] = float(abs(d) / sig) if sig > 0 else float("inf")
+                series["plaquette"].append(1.0 - e.EnergyMag() / nplaq)
+                t, s = e.PlaqExp()
+                series["plaquette_t"].append(1.0 - t / nt if nt else float("nan"))
+                series["plaquette_s"].append(1.0 - s / ns if ns else float("nan"))
+                series["polyakov"].append(e.PolyakovLoop())
+                series["wilson"].append(e.WilsonLoop())
+            r = {"acceptance": acc / max(1, ntraj), "seconds": time.perf_counter() - t0}
+            for k in obs:
+                r[k] = float(np.mean(series[k]))
+                r[k + "_err"] = _binned_error(np.array(series[k]))
+            res[prec] = r
+    # FP32 minus FP64 for each observable, in units of the combined binned error
+    for k in obs:
+        d = res["fp32"][k] - res["fp64"][k]
+        sig = float(np.hypot(res["fp32"][k + "_err"], res["fp64"][k + "_err"]))
+        res[k + "_diff"] = d
+        res[k + "_diff_in_sigma"] = float(abs(d) / sig) if sig > 0 else float("inf")
     return res
 
 

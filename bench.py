@@ -41,14 +41,14 @@ sys.path.insert(0, ROOT)
 CONFIGS = {
     # name: nc, dims, beta, dt, level, md steps per trajectory
     "su3_32": dict(nc=3, dims=[32, 32, 32, 32], beta=6.0, dt=0.02, level=6, nsteps=50),
-    "su8_10": dict(nc=8, dims=[10, 10, 10, 10], beta=20.0, dt=0.01, level=8, nsteps=100),
+    "su8_10": dict(nc=8, dims=[10, 10, 10, 10], beta=20.0, dt=0.01, level=8, nsteps=100, ensemble=60),
     "su3_8": dict(nc=3, dims=[8, 8, 8, 8], beta=5.70, dt=0.02, level=8, nsteps=50),
     # large NC: every complex product of the FP32 path on the tensor cores (split TF32 x 3);
     # the CPU sample runs the same colour number on a smaller lattice (per-link rates)
     "su32_8": dict(nc=32, dims=[8, 8, 8, 8], beta=2048.0, dt=0.005, level=8, nsteps=20, tensor=True,
-                   cpu_dims=[2, 2, 2, 2]),
+                   cpu_dims=[2, 2, 2, 2], ensemble=20),
     "su64_4x16": dict(nc=64, dims=[4, 16, 16], beta=8192.0, dt=0.005, level=8, nsteps=20, tensor=True,
-                      cpu_dims=[2, 2, 4]),
+                      cpu_dims=[2, 2, 4], ensemble=20),
 }
 
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
@@ -73,6 +73,16 @@ def tf32_peak():
             return 0.5 * float(json.load(f)["bf16_tflops"]), "measured bf16 / 2"
     except Exception:
         return 0.5 * FALLBACK_BF16_TFLOPS, "fallback bf16 / 2"
+
+
+def fp32_peak(device):
+    """Measured FP32 FFMA peak of the device, TFLOP/s (askja_peak_flops)."""
+    import ctypes
+
+    import askja_b200 as ab
+    g = ctypes.c_double()
+    rc = ab.library().askja_peak_flops(int(device), 0, 5, ctypes.byref(g))
+    return g.value / 1e3 if rc == 0 else float("nan")
 
 
 def tensor_products_per_link(dim, level, reunit=True):
@@ -289,8 +299,21 @@ def run_ours(args):
                     "traffic": None, "flops_per_launch": fpl * links, "avg_launch_ms": f32["kernel_ms"],
                     "complex_tflops": 8 * nc ** 3 * tensor_products_per_link(len(dims), cfg["level"]) * links
                     / sec / 1e12}
+    elif f32["tuning"]["path"] == 1 or (f32["tuning"]["path"] is None and nc > 4):
+        # row-per-thread kernels (NC >= 5): bound by the FP32 FMA pipe; flops per link =
+        # 8 NC^3 x (4(D-1) + 1 force products + LEVEL Horner products), against the FFMA peak
+        # measured on this device now
+        order = cfg["level"] if 0 <= cfg["level"] <= 8 else 8
+        fpl = 8 * nc ** 3 * (4 * (len(dims) - 1) + 1 + order)
+        pk = fp32_peak(dev)
+        tflops = fpl * links / (f32["kernel_ms"] / 1e3) / 1e12
+        roofline = {"bound": "fp32", "kernel": f"fused kick+drift (rows::k_force<{nc},float,1>)",
+                    "achieved": tflops, "peak": pk, "unit": "TFLOP/s", "frac": tflops / pk,
+                    "peak_source": "measured FFMA on this device (askja_peak_flops)", "traffic": None,
+                    "flops_per_launch": fpl * links, "avg_launch_ms": f32["kernel_ms"],
+                    "hbm_achieved_gbs": achieved}
     else:
-        roofline = {"bound": "hbm", "kernel": "fused kick+drift (small::k_force<3,float,1>)",
+        roofline = {"bound": "hbm", "kernel": f"fused kick+drift (small::k_force<{nc},float,1>)",
                     "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                     "peak_source": peak_kind, "traffic": traffic,
                     "bytes_per_launch": bytes_per_lu * links, "avg_launch_ms": f32["kernel_ms"]}
@@ -346,6 +369,10 @@ def precision_report(cfg, dev):
     r = precision.compare(nc, dims, cfg["beta"], cfg["dt"], cfg["level"], cfg["nsteps"], u0, ntraj_dh=3,
                           device=dev)
     r["thermalisation_trajectories"] = therm
+    if cfg.get("ensemble"):
+        # observables of independent FP32 and FP64 chains from the same start
+        r["ensemble"] = precision.ensemble(nc, dims, cfg["beta"], cfg["dt"], cfg["level"], cfg["nsteps"], u0,
+                                           ntraj=cfg["ensemble"], device=dev)
     return r
 
 

@@ -211,3 +211,9 @@ def test_precision_module_small():
     ens = precision.ensemble(nc, dims, beta, dt, level, n, u0, 10)
     # a few trajectories from a hot start: far from equilibrium, but moving up from 0
     assert 0.05 < ens["fp64"]["plaquette"] < 0.8 and 0.05 < ens["fp32"]["plaquette"] < 0.8
+    # temporal and spatial planes average to the whole (3 of each in D = 4)
+    for k in ("fp64", "fp32"):
+        e = ens[k]
+        assert e["plaquette"] == pytest.approx(0.5 * (e["plaquette_t"] + e["plaquette_s"]), rel=1e-12)
+        assert abs(e["wilson"]) <= 1.0 + 1e-12
+    assert abs(ens["plaquette_t_diff"]) < 0.05 and abs(ens["wilson_diff"]) < 0.5
