@@ -39,7 +39,7 @@ EXPORTS = [
     "askja_updateUandcopyDown", "askja_copyDown", "askja_takeconfiguration", "askja_loadconfiguration",
     "askja_reunitarise", "askja_EnergyMag", "askja_simpleenergyEl", "askja_EnergyEl", "askja_TotalEnergy",
     "askja_GaussLaw", "askja_UViol", "askja_WilsonLoop", "askja_PolyakovLoop", "askja_WilsonLoopDir",
-    "askja_PlaqExp", "askja_scalarLoopcorr", "askja_trajectory", "askja_run_trajectories", "askja_leapfrog",
+    "askja_PlaqExp", "askja_scalarLoopcorr", "askja_eigenphases", "askja_trajectory", "askja_run_trajectories", "askja_leapfrog",
     "askja_md_steps", "askja_params_load", "askja_params_store", "askja_file_stem", "askja_conf_write",
     "askja_conf_read", "askja_host_alloc", "askja_host_free", "askja_plaqexp_static", "askja_peak_flops",
     "askja_batch_create", "askja_batch_destroy", "askja_batch_last_error", "askja_batch_stream",
@@ -122,6 +122,7 @@ def library() -> ctypes.CDLL:
     L.askja_simpleenergyEl.argtypes = [vp, ip, dp]
     L.askja_WilsonLoopDir.argtypes = [vp, ip, dp]
     L.askja_PlaqExp.argtypes = [vp, dp, dp]
+    L.askja_eigenphases.argtypes = [vp, dp, dp]
     L.askja_trajectory.argtypes = [vp, ip, ctypes.POINTER(TrajResult)]
     L.askja_run_trajectories.argtypes = [vp, ip, ip, ip, ctypes.POINTER(TrajResult), dp]
     L.askja_leapfrog.argtypes = [vp, ip, ctypes.c_double]
@@ -299,6 +300,13 @@ class Engine:
         t, s = ctypes.c_double(), ctypes.c_double()
         self._ck(self.lib.askja_PlaqExp(self._ctx, ctypes.byref(t), ctypes.byref(s)))
         return t.value, s.value
+
+    def eigenphases(self):
+        """getevs (measurements4d.cpp:185-309): averaged sorted eigenphases of
+        the Wilson lines (direction 1) and the Polyakov lines (direction 0)."""
+        w, p = np.zeros(self.nc), np.zeros(self.nc)
+        self._ck(self.lib.askja_eigenphases(self._ctx, _dptr(w), _dptr(p)))
+        return w, p
 
     def scalarLoopcorr(self):
         out = np.zeros(self.dims[0])

@@ -3,6 +3,7 @@
 Produces
   askja_b200/libaskja_b200.so   the C-ABI library (include/askja_gpu.h)
   askja_b200/askja              the command-line driver (drop-in for ./askja)
+  askja_b200/measure4d          the measurement driver (drop-in for ./measure4d)
 
 CUDA sources are compiled for sm_100a only
 (``-gencode arch=compute_100a,code=sm_100a``); the CUDA runtime is linked
@@ -21,6 +22,7 @@ CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libaskja_b200.so")
 EXE = os.path.join(HERE, "askja")
+MEASURE = os.path.join(HERE, "measure4d")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 # the image exports CXX pointing at a wrapper without OpenMP specs; the system g++ is used
 CXX = "g++"
@@ -30,7 +32,7 @@ NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xco
                   "--expt-relaxed-constexpr", "-ccbin", CXX]
 CU_SOURCES = ["kernels_fp64.cu", "kernels_fp32.cu", "engine.cu", "static_plaq.cu", "peak.cu", "batch.cu"]
 CPP_SOURCES = ["hostio.cpp"]
-HEADERS = ["common.cuh", "small.cuh", "rows.cuh", "misc.cuh", "kernels.cuh", "launch.h", "batch.cuh", "tc.cuh"]
+HEADERS = ["common.cuh", "small.cuh", "rows.cuh", "misc.cuh", "kernels.cuh", "launch.h", "batch.cuh", "tc.cuh", "eig.cuh"]
 
 
 def _newer(target: str, deps) -> bool:
@@ -79,10 +81,12 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
     if _newer(LIB, objs):
         cmd = [NVCC] + ARCH + ["-shared", "-ccbin", CXX, "-o", LIB] + objs + ["-cudart", "static"]
         subprocess.check_call(cmd)
-    main_src = os.path.join(CSRC, "askja_main.cpp")
-    if _newer(EXE, [main_src, LIB, os.path.join(ROOT, "include", "askja_gpu.h")]):
-        subprocess.check_call([CXX, "-O2", "-std=c++17", main_src, "-o", EXE, "-L" + HERE, "-laskja_b200",
-                               "-Wl,-rpath,$ORIGIN"])
+    libdir = os.path.dirname(LIB)
+    for src, exe in (("askja_main.cpp", EXE), ("measure4d_main.cpp", MEASURE)):
+        main_src = os.path.join(CSRC, src)
+        if _newer(exe, [main_src, LIB, os.path.join(ROOT, "include", "askja_gpu.h")]):
+            subprocess.check_call([CXX, "-O2", "-std=c++17", main_src, "-o", exe, "-L" + libdir, "-laskja_b200",
+                                   "-Wl,-rpath,$ORIGIN"])
     return LIB
 
 

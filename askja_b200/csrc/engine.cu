@@ -14,6 +14,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
 #include <cmath>
 #include <map>
 #include <mutex>
@@ -55,6 +56,8 @@ struct askja_ctx {
   double* partial = nullptr;
   double* sums = nullptr;   // [0..1] plaq t/s, [2..4] link sums, [5] gauss, [6..] line results
   double* lines = nullptr;  // per-line results
+  double2* eigs = nullptr;  // eigenvalues of the N0 + N1 lines of askja_eigenphases
+  int* eigfail = nullptr;
   TrajState* st = nullptr;
   double* logbuf = nullptr;
   int logcap = 0;
@@ -252,7 +255,7 @@ void askja_destroy(askja_ctx* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   drop_graphs(c);
   void* bufs[] = {c->U[0], c->U[1], c->P, c->P2, c->Uconf, c->nbr, c->partial, c->sums, c->lines,
-                  c->st,   c->logbuf, c->staging, c->nonfinite, c->tc_status};
+                  c->st,   c->logbuf, c->staging, c->nonfinite, c->tc_status, c->eigs, c->eigfail};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -327,6 +330,10 @@ int askja_create(const askja_params* p, askja_ctx** out) {
   long maxlines = 1;
   for (int i = 0; i < p->dim; i++) maxlines = std::max(maxlines, (long)p->n[i]);
   CKC(cudaMalloc(&c->lines, (maxlines + 8) * sizeof(double)));
+  if (p->dim >= 2) {
+    CKC(cudaMalloc(&c->eigs, (size_t)(p->n[0] + p->n[1]) * p->nc * sizeof(double2)));
+    CKC(cudaMalloc(&c->eigfail, sizeof(int)));
+  }
   CKC(cudaMalloc(&c->st, sizeof(TrajState)));
   CKC(cudaMemset(c->st, 0, sizeof(TrajState)));
   c->logcap = 4096;
@@ -582,6 +589,47 @@ int askja_WilsonLoopDir(askja_ctx* c, int dir, double* out) {
   if (int rc = check_ctx(c)) return rc;
   if (!out || dir < 1 || dir >= c->D) return set_err(c, ASKJA_ERR_ARG, "WilsonLoopDir needs 1 <= dir < DIM");
   return line_mean(c, dir, c->lat.n[0], c->lat.stride[0], out);
+}
+
+int askja_eigenphases(askja_ctx* c, double* w, double* p) {
+  if (int rc = check_ctx(c)) return rc;
+  if (!w || !p) return set_err(c, ASKJA_ERR_ARG, "null output");
+  if (c->D < 2) return set_err(c, ASKJA_ERR_ARG, "eigenphases need DIM >= 2");
+  DevGuard g(c->p.device);
+  const int N = c->N, n0 = c->lat.n[0], n1 = c->lat.n[1];
+  CK(cudaMemsetAsync(c->eigfail, 0, sizeof(int), c->stream));
+  // Wilson lines along direction 1 through (x0, 0, ..), Polyakov lines along 0 through (0, x1, 0, ..)
+  KL(c->ks->line_eigs(c->lc, cur_u(c), 1, n0, c->lat.stride[0], c->eigs, c->eigfail), "line eigenvalues");
+  KL(c->ks->line_eigs(c->lc, cur_u(c), 0, n1, c->lat.stride[1], c->eigs + (size_t)n0 * N, c->eigfail),
+     "line eigenvalues");
+  std::vector<double2> ev((size_t)(n0 + n1) * N);
+  int fail = 0;
+  CK(cudaMemcpyAsync(ev.data(), c->eigs, ev.size() * sizeof(double2), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(&fail, c->eigfail, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (fail) return set_err(c, ASKJA_ERR_CUDA, "line eigenvalues did not converge");
+  // per line: phases, re-centred by the winding when |winding| > 0.1, sorted, summed; then averaged
+  const double pi = 3.14159265358979323846;
+  std::vector<double> ph(N);
+  for (int i = 0; i < N; i++) w[i] = p[i] = 0.0;
+  for (int q = 0; q < n0 + n1; q++) {
+    double winding = 0.0;
+    for (int i = 0; i < N; i++) {
+      const double2 z = ev[(size_t)q * N + i];
+      ph[i] = std::atan2(z.y, z.x);
+      winding += ph[i] / (2 * pi);
+    }
+    if (winding > 0.1 || winding < -0.1)
+      for (int i = 0; i < N; i++) ph[i] -= winding * 2 * pi / N;
+    std::sort(ph.begin(), ph.end());
+    double* acc = q < n0 ? w : p;
+    for (int i = 0; i < N; i++) acc[i] += ph[i];
+  }
+  for (int i = 0; i < N; i++) {
+    w[i] /= n0;
+    p[i] /= n1;
+  }
+  return ASKJA_OK;
 }
 
 int askja_scalarLoopcorr(askja_ctx* c, double* out) {

@@ -8,6 +8,7 @@
 #include "misc.cuh"
 #include "rows.cuh"
 #include "small.cuh"
+#include "eig.cuh"
 #include "tc.cuh"
 
 namespace askja {
@@ -321,6 +322,19 @@ cudaError_t slice_trace(const LaunchCtx& c, const void* U, double* out) {
 }
 
 template <typename T>
+cudaError_t line_eigs(const LaunchCtx& c, const void* U, int dir, int nlines, int start_stride, double2* ev,
+                      int* fail) {
+  using S2 = typename Storage<T>::type;
+  const int N = c.lat.N;
+  const size_t smem = 2 * (size_t)N * N * sizeof(cpx<double>);
+  auto k = eig::k_line_eigs<S2>;
+  cudaError_t e;
+  if ((e = set_smem(k, smem)) != cudaSuccess) return e;
+  k<<<nlines, std::max(32, (N + 31) / 32 * 32), smem, c.stream>>>(c.lat, (const S2*)U, dir, start_stride, ev, fail);
+  return cudaGetLastError();
+}
+
+template <typename T>
 cudaError_t refresh(const LaunchCtx& c, void* P, uint64_t seed, const unsigned long long* traj_dev,
                     unsigned long long traj_host, double scale) {
   using S2 = typename Storage<T>::type;
@@ -368,7 +382,7 @@ cudaError_t to_conf(const LaunchCtx& c, const void* f, void* conf) {
 template <typename T>
 constexpr KernelSet make_set() {
   return KernelSet{&force<T>,   &drift<T>,   &reunit<T>,  &plaq<T>,           &linksums<T>,  &gauss<T>, &lines<T>,
-                   &slice_trace<T>, &refresh<T>, &identity<T>, &gauss_matrices<T>, &from_conf<T>, &to_conf<T>};
+                   &slice_trace<T>, &line_eigs<T>, &refresh<T>, &identity<T>, &gauss_matrices<T>, &from_conf<T>, &to_conf<T>};
 }
 
 }  // namespace detail

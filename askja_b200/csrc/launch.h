@@ -45,6 +45,9 @@ struct KernelSet {
   cudaError_t (*gauss)(const LaunchCtx&, const void* U, const void* Pi, double* partial, double* out);
   cudaError_t (*lines)(const LaunchCtx&, const void* U, int dir, int nlines, int start_stride, double* out);
   cudaError_t (*slice_trace)(const LaunchCtx&, const void* U, double* out);
+  // eigenvalues of closed line matrices: ev[q*NC + i] (complex), *fail set on no convergence
+  cudaError_t (*line_eigs)(const LaunchCtx&, const void* U, int dir, int nlines, int start_stride, double2* ev,
+                           int* fail);
   cudaError_t (*refresh)(const LaunchCtx&, void* P, uint64_t seed, const unsigned long long* traj_dev,
                          unsigned long long traj_host, double scale);
   cudaError_t (*identity)(const LaunchCtx&, void* U);

@@ -131,6 +131,14 @@ ASKJA_API int askja_PolyakovLoop(askja_ctx* ctx, double* out);                 /
 ASKJA_API int askja_WilsonLoopDir(askja_ctx* ctx, int dir, double* out);       /* measurements4d.cpp:311-355 */
 ASKJA_API int askja_PlaqExp(askja_ctx* ctx, double* temporal, double* spatial);/* measurements4d.cpp:885-927 */
 ASKJA_API int askja_scalarLoopcorr(askja_ctx* ctx, double* out /* N0 values */); /* measurements4d.cpp:357-408 */
+/* getevs (measurements4d.cpp:185-309): eigenphases of the N0 Wilson lines
+ * along direction 1 through (x0,0,..) and of the N1 Polyakov lines along
+ * direction 0 through (0,x1,0,..); per line the NC phases arg(lambda) are
+ * re-centred by the winding (sum/2pi) when it exceeds 0.1 in magnitude and
+ * sorted; w[i] and p[i] are the i-th sorted phase averaged over the lines
+ * (NC values each).  Eigenvalues on the GPU (Hessenberg + shifted QR in
+ * FP64), the sort and average on the host.  DIM >= 2. */
+ASKJA_API int askja_eigenphases(askja_ctx* ctx, double* w, double* p);
 
 /* ---- whole trajectories, on the device -------------------------------- */
 /* One HMC trajectory as in sun.cpp:1249-1318 with `nsteps` link updates:
