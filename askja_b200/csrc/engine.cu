@@ -735,7 +735,7 @@ int askja_set_tuning(askja_ctx* c, const askja_tuning* t) {
     return set_err(c, ASKJA_ERR_ARG, "invalid tuning");
   c->lc.force_rows = t->path;
   c->lc.rows_groups = t->groups;
-  c->lc.small_occ = t->occupancy ? 1 : 0;
+  c->lc.small_occ = t->occupancy < 0 ? 0 : t->occupancy > 2 ? 2 : t->occupancy;
   drop_graphs(c);
   return ASKJA_OK;
 }
@@ -752,6 +752,7 @@ int askja_autotune(askja_ctx* c, int reps, askja_tuning* out) {
   if (c->N <= 4) {
     cands.push_back({0, 0, 0});
     cands.push_back({0, 0, 1});
+    cands.push_back({0, 0, 2});
   }
   if (askja::tc_supported(c->N, c->D, fp64)) cands.push_back({2, 0, 0});
   std::vector<int> seen;

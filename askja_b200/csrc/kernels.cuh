@@ -91,7 +91,14 @@ cudaError_t small_force(const LaunchCtx& c, int mode, const void* U, const void*
   const int threads = 32 * std::min(c.lat.D, 4);
   const S2* u = (const S2*)U;
   const S2* pi = (const S2*)Pin;
-  if (c.small_occ) {
+  if (c.small_occ == 2) {
+    if (mode == 0)
+      small::k_force_occ<N, T, S2, 0, 2><<<grid, threads, 0, c.stream>>>(c.lat, u, pi, (S2*)Pout, (S2*)Uout, (T)ek,
+                                                                           (T)ed, c.order, c.reunit);
+    else
+      small::k_force_occ<N, T, S2, 1, 2><<<grid, threads, 0, c.stream>>>(c.lat, u, pi, (S2*)Pout, (S2*)Uout, (T)ek,
+                                                                           (T)ed, c.order, c.reunit);
+  } else if (c.small_occ) {
     if (mode == 0)
       small::k_force_occ<N, T, S2, 0><<<grid, threads, 0, c.stream>>>(c.lat, u, pi, (S2*)Pout, (S2*)Uout, (T)ek,
                                                                         (T)ed, c.order, c.reunit);

@@ -18,7 +18,7 @@ struct LaunchCtx {
   int force_rows;   // kernel mapping: 0 thread-per-link (NC <= 4), 1 row-per-thread,
                     // 2 tensor cores (FP32, NC = 32 or 64, DIM >= 2)
   int rows_groups;  // row kernels: sites per CTA (0: default 128/NC)
-  int small_occ;    // thread-per-link kernels: 1 = higher-occupancy register budget
+  int small_occ;    // thread-per-link kernels: register budget for 0 default, 1 / 2 more resident CTAs
   void* scratch;    // tensor-core path: per-link contiguous copy of U (V*D*NC*NC float2)
   unsigned* status; // tensor-core path: nonzero after a bounded wait gave up
   // row-kernel reunitarisation: run only when *gate % gate_every == 0 (null: always)

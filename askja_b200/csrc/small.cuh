@@ -428,9 +428,10 @@ __global__ void __launch_bounds__(128) k_force(Lat L, const S2* __restrict__ U, 
 }
 
 // The same kernel with a tighter register budget for more resident CTAs
-// (6 per SM in FP32, 3 in FP64); the autotuner picks it where it is faster.
-template <int N, typename T, typename S2, int MODE>
-__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 6 : 3)
+// (OCC = 1: 6 per SM in FP32, 3 in FP64; OCC = 2: 7 / 4); the autotuner picks
+// the budget where it is faster.
+template <int N, typename T, typename S2, int MODE, int OCC = 1>
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 5 + OCC : 2 + OCC)
     k_force_occ(Lat L, const S2* __restrict__ U, const S2* Pin, S2* Pout, S2* __restrict__ Uout, T eps_k, T eps_d,
                 int order, int reunit) {
   const int x = blockIdx.x * 32 + (threadIdx.x & 31);

@@ -138,3 +138,20 @@ def test_path_validation():
     with ab.Engine(32, [2, 2], beta=1.0, precision="fp64") as e:
         with pytest.raises(ab.AskjaError):
             ab.set_tuning(e, {"path": 2})
+
+
+def test_trajectories_stay_unitary_with_gated_gram_schmidt():
+    """Tensor-core trajectories (graph replays): the link update keeps U' as
+    unitary as U and the engine re-orthonormalises U before every 10th
+    trajectory, so the defect stays at FP32 rounding over many trajectories."""
+    nc, dims = 32, [2, 2, 2]
+    O, u, pi, beta = setup(nc, dims, 5)
+    with ab.Engine(nc, dims, beta=beta, dt=0.005, level=8, precision="fp32", kernel_path=2, seed=3) as e:
+        e.set_links(u)
+        last, log = e.run_trajectories(12, 10, use_graph=True)
+        assert last["n_tot"] == 12
+        assert np.all(np.isfinite(log))
+        assert unitarity(e.get_links()) < 3e-6
+        assert unitarity(e.get_saved_links()) < 3e-6
+        # dH stays small at this step size
+        assert np.abs(log[:, 2]).max() < 1.0
