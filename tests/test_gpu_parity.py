@@ -6,12 +6,14 @@ update, action, kinetic sums and one leapfrog trajectory (it is not bit-exact:
 reduction order and the factoring of the staple product differ).  The FP32
 path is checked against the same FP64 answers with FP32-level tolerances
 (relative 2e-5 on fields, 1e-6 relative on the FP64-accumulated sums)."""
+import os
+
 import numpy as np
 import pytest
 
 import askja_b200 as ab
 from conftest import rel
-from oracle import Oracle, fields
+from oracle import Oracle, Reference, fields
 
 pytestmark = pytest.mark.gpu
 
@@ -198,3 +200,53 @@ def test_large_nc_vs_oracle(nc, dims, precision):
             uu = O.updateU(uu, pp, 0.005, 8)
             pp = O.updateE(uu, pp, 0.005 if k < 1 else 0.0025)
         assert rel(e.get_links(), uu) < (TOL64 if precision == "fp64" else 5e-6)
+
+
+@pytest.mark.skipif(not Reference.available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("start", ["cold", "hot"])
+def test_config1_step_by_step_vs_reference(start):
+    """SU(3) 8^4, BETA=5.70, DT=0.02, LEVEL=8, 50 leapfrog steps: the FP64
+    engine and the reference's own sun.cpp routines (the shim-built harness)
+    take the same U and P and the same updateE / updateUandcopyDown sequence
+    (sun.cpp:1174-1250); links, momenta and H agree after every step.  The
+    Metropolis decision itself uses each side's own random stream."""
+    nc, dims, beta, dt, level, nsteps = 3, [8, 8, 8, 8], 5.70, 0.02, 8, 50
+    rng = np.random.default_rng(1 if start == "cold" else 2)
+    O = Oracle(nc, dims)
+    nl = O.vol * O.dim
+    if start == "cold":
+        u = np.broadcast_to(np.eye(nc, dtype=np.complex128), O.shape).copy()
+    else:
+        u = fields.haar(nc, nl, rng).reshape(O.shape)
+    pi = fields.momenta(nc, nl, beta, rng, O)
+    R = Reference(nc, dims, beta=beta, level=level)
+    R.threads(os.cpu_count() or 1)
+    for name in ("u", "U"):
+        R.set(name, u)
+    R.set("pi", pi)
+    R.set("Pi", pi)
+
+    def ham(emag, k):
+        return beta * (emag + k / (2 * nc))
+
+    with ab.Engine(nc, dims, beta=beta, dt=dt, level=level) as e:
+        e.set_links(u)
+        e.set_momenta(pi, 0)
+        h0_ref = ham(R.EnergyMag(), R.simpleenergyEl("pi"))
+        assert e.hamiltonian(0) == pytest.approx(h0_ref, rel=1e-13)
+        R.updateE(0.5 * dt)
+        e.updateE(0.5 * dt)
+        for k in range(nsteps):
+            R.updateUandcopyDown(dt)
+            e.updateUandcopyDown(dt)
+            last = k == nsteps - 1
+            R.updateE(0.5 * dt if last else dt)
+            e.updateE(0.5 * dt if last else dt)
+            assert rel(e.get_links(), R.get("u")) < 1e-11, k
+            assert rel(e.get_momenta(1), R.get("Pi")) < 1e-11, k
+        h1_ref = ham(R.EnergyMag(), R.simpleenergyEl("Pi"))
+        h1 = beta * (e.EnergyMag() + e.simpleenergyEl(1) / (2 * nc))
+        assert h1 == pytest.approx(h1_ref, rel=1e-12)
+        assert abs((h1 - h0_ref) - (h1_ref - h0_ref)) < 1e-8
+        t, s = e.PlaqExp()
+        assert t + s == pytest.approx(R.EnergyMag(), rel=1e-12)
