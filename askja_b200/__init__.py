@@ -44,7 +44,7 @@ EXPORTS = [
     "askja_conf_read", "askja_host_alloc", "askja_host_free", "askja_plaqexp_static", "askja_peak_flops",
     "askja_batch_create", "askja_batch_destroy", "askja_batch_last_error", "askja_batch_stream",
     "askja_batch_hot_start", "askja_batch_set_links", "askja_batch_get_links", "askja_batch_run",
-    "askja_batch_plaquette", "askja_autotune", "askja_set_tuning",
+    "askja_batch_plaquette", "askja_autotune", "askja_set_tuning", "askja_set_links_async", "askja_trajectory_async",
 ]
 
 
@@ -108,7 +108,7 @@ def library() -> ctypes.CDLL:
     for name in ("askja_sync", "askja_initializeU", "askja_copyDown", "askja_takeconfiguration",
                  "askja_loadconfiguration", "askja_reunitarise"):
         getattr(L, name).argtypes = [vp]
-    for name in ("askja_set_links", "askja_get_links", "askja_get_saved_links"):
+    for name in ("askja_set_links", "askja_set_links_async", "askja_get_links", "askja_get_saved_links"):
         getattr(L, name).argtypes = [vp, vp]
     for name in ("askja_set_momenta", "askja_get_momenta"):
         getattr(L, name).argtypes = [vp, ip, vp]
@@ -124,6 +124,7 @@ def library() -> ctypes.CDLL:
     L.askja_PlaqExp.argtypes = [vp, dp, dp]
     L.askja_eigenphases.argtypes = [vp, dp, dp]
     L.askja_trajectory.argtypes = [vp, ip, ctypes.POINTER(TrajResult)]
+    L.askja_trajectory_async.argtypes = [vp, ip, vp]
     L.askja_run_trajectories.argtypes = [vp, ip, ip, ip, ctypes.POINTER(TrajResult), dp]
     L.askja_leapfrog.argtypes = [vp, ip, ctypes.c_double]
     L.askja_md_steps.argtypes = [vp, ip, ctypes.c_double]
@@ -215,6 +216,11 @@ class Engine:
     def set_links_ptr(self, ptr: int):
         """Upload links from a raw host pointer (e.g. pinned memory)."""
         self._ck(self.lib.askja_set_links(self._ctx, ctypes.c_void_p(ptr)))
+
+    def set_links_async(self, ptr: int):
+        """askja_set_links_async from a raw (page-locked) host pointer: the copy
+        overlaps the work already enqueued; see include/askja_gpu.h."""
+        self._ck(self.lib.askja_set_links_async(self._ctx, ctypes.c_void_p(ptr)))
 
     def get_links(self):
         out = np.empty(self.shape, np.complex128)
@@ -322,6 +328,12 @@ class Engine:
         r = TrajResult()
         self._ck(self.lib.askja_trajectory(self._ctx, int(nsteps), ctypes.byref(r)))
         return r.as_dict()
+
+    def trajectory_async(self, nsteps: int, out_ptr: int = 0):
+        """askja_trajectory_async: enqueue a trajectory (graph replay) and the
+        copy of its outcome to out_ptr (a page-locked TrajResult, or 0);
+        valid after sync()."""
+        self._ck(self.lib.askja_trajectory_async(self._ctx, int(nsteps), ctypes.c_void_p(out_ptr or None)))
 
     def run_trajectories(self, ntraj: int, nsteps: int, use_graph: bool = True, want_log: bool = True):
         r = TrajResult()

@@ -65,6 +65,16 @@ struct askja_ctx {
   unsigned long long* nonfinite = nullptr;
   unsigned* tc_status = nullptr;  // tensor-core kernels: set when a bounded wait gave up
   cudaStream_t stream = nullptr;
+  // askja_set_links_async: copy stream and two device staging buffers, used in
+  // turn; up_copied[b] marks the copy into up[b] done, up_free[b] the
+  // conversion out of it; up_bad counts non-finite input values until the
+  // next synchronisation
+  cudaStream_t copy_stream = nullptr;
+  void* up[2] = {nullptr, nullptr};
+  cudaEvent_t up_copied[2] = {nullptr, nullptr};
+  cudaEvent_t up_free[2] = {nullptr, nullptr};
+  int up_next = 0;
+  unsigned long long* up_bad = nullptr;
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
   int g_nsteps[2] = {-1, -1};
   std::string err;
@@ -141,6 +151,29 @@ int launch_ok(askja_ctx* c, cudaError_t e, const char* what) {
 // tensor-core path: trajectories between two Gram-Schmidt passes over U
 constexpr int TC_REUNIT_EVERY = 10;
 
+bool paired(const askja_ctx* c) { return c->lc.force_rows == 3; }
+
+// Site-pair mapping: the fused kick+drift launches run on the site-pair
+// layout of the current links and of P; this converts both, in place, before
+// (and again after) a run of such launches.  A no-op for the other mappings.
+int pair_layout(askja_ctx* c, void* P) {
+  if (!paired(c)) return ASKJA_OK;
+  KL(c->ks->pair_swap(c->lc, cur_u(c)), "site-pair layout");
+  KL(c->ks->pair_swap(c->lc, P), "site-pair layout");
+  return ASKJA_OK;
+}
+
+// n fused kick+drift launches: the first kicks by first_kick, the others by dt
+int fused_steps(askja_ctx* c, int n, double first_kick, double dt) {
+  if (n <= 0) return ASKJA_OK;
+  if (int rc = pair_layout(c, c->P)) return rc;
+  for (int i = 0; i < n; i++) {
+    KL(c->ks->force(c->lc, 1, cur_u(c), c->P, c->P, c->U[1 - c->cur], i == 0 ? first_kick : dt, dt), "kick+drift");
+    c->cur ^= 1;
+  }
+  return pair_layout(c, c->P);
+}
+
 // Enqueue one whole trajectory (no host synchronisation; graph-capturable).
 int enqueue_trajectory(askja_ctx* c, int nsteps) {
   const double dt = c->p.dt;
@@ -161,10 +194,7 @@ int enqueue_trajectory(askja_ctx* c, int nsteps) {
   KL(c->ks->linksums(c->lc, c->P, nullptr, nullptr, c->partial, c->sums + 2), "kinetic");
   askja::misc::k_energy<<<1, 1, 0, c->stream>>>(c->sums, c->p.beta, c->N, &c->st->h_old);
   KL(cudaGetLastError(), "energy");
-  for (int i = 0; i < nsteps; i++) {
-    KL(c->ks->force(c->lc, 1, cur_u(c), c->P, c->P, c->U[1 - c->cur], i == 0 ? 0.5 * dt : dt, dt), "kick+drift");
-    c->cur ^= 1;
-  }
+  if (int rc = fused_steps(c, nsteps, 0.5 * dt, dt)) return rc;
   KL(c->ks->force(c->lc, 0, cur_u(c), c->P, c->P, nullptr, 0.5 * dt, 0.0), "kick");
   KL(c->ks->plaq(c->lc, cur_u(c), c->partial, c->sums), "plaq");
   KL(c->ks->linksums(c->lc, c->P, nullptr, nullptr, c->partial, c->sums + 2), "kinetic");
@@ -188,6 +218,14 @@ void drop_graphs(askja_ctx* c) {
 // bounded wait (its outputs are incomplete)
 int sync_checked(askja_ctx* c) {
   CK(cudaStreamSynchronize(c->stream));
+  if (c->up_bad) {
+    unsigned long long bad = 0;
+    CK(cudaMemcpy(&bad, c->up_bad, sizeof bad, cudaMemcpyDeviceToHost));
+    if (bad) {
+      CK(cudaMemset(c->up_bad, 0, sizeof bad));
+      return set_err(c, ASKJA_ERR_NONFINITE, "an asynchronous upload held %llu non-finite values", bad);
+    }
+  }
   if (c->lc.force_rows == 2) {
     unsigned st = 0;
     CK(cudaMemcpy(&st, c->tc_status, sizeof st, cudaMemcpyDeviceToHost));
@@ -253,7 +291,15 @@ void askja_destroy(askja_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->p.device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
   drop_graphs(c);
+  for (int b = 0; b < 2; b++) {
+    if (c->up[b]) cudaFree(c->up[b]);
+    if (c->up_copied[b]) cudaEventDestroy(c->up_copied[b]);
+    if (c->up_free[b]) cudaEventDestroy(c->up_free[b]);
+  }
+  if (c->up_bad) cudaFree(c->up_bad);
+  if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
   void* bufs[] = {c->U[0], c->U[1], c->P, c->P2, c->Uconf, c->nbr, c->partial, c->sums, c->lines,
                   c->st,   c->logbuf, c->staging, c->nonfinite, c->tc_status, c->eigs, c->eigfail};
   for (void* b : bufs)
@@ -278,10 +324,13 @@ int askja_create(const askja_params* p, askja_ctx** out) {
   if (!(p->beta > 0.0) || !std::isfinite(p->beta)) return set_err(nullptr, ASKJA_ERR_ARG, "BETA must be > 0");
   if (p->precision != ASKJA_FP64 && p->precision != ASKJA_FP32)
     return set_err(nullptr, ASKJA_ERR_ARG, "unknown precision %d", p->precision);
-  if (p->kernel_path < 0 || p->kernel_path > 2)
+  if (p->kernel_path < 0 || p->kernel_path > 3)
     return set_err(nullptr, ASKJA_ERR_ARG, "unknown kernel path %d", p->kernel_path);
   if (p->kernel_path == 2 && !askja::tc_supported(p->nc, p->dim, p->precision == ASKJA_FP64))
     return set_err(nullptr, ASKJA_ERR_ARG, "tensor-core path needs FP32, NC = 32 or 64 and DIM >= 2");
+  if (p->kernel_path == 3 && !askja::pair_supported(p->nc, p->dim, p->precision == ASKJA_FP64, p->n[p->dim - 1]))
+    return set_err(nullptr, ASKJA_ERR_ARG, "site-pair path needs FP32, NC = 3, DIM >= 2 and an even N%d",
+                   p->dim - 1);
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
     return set_err(nullptr, ASKJA_ERR_NODEVICE, "no CUDA device available (the engine has no CPU fallback)");
@@ -358,7 +407,8 @@ int askja_create(const askja_params* p, askja_ctx** out) {
   if (p->kernel_path == 0) {
     std::lock_guard<std::mutex> lock(g_tune_mutex);
     auto it = g_tune_cache.find(std::make_tuple(p->nc, p->dim, p->precision));
-    if (it != g_tune_cache.end()) {
+    if (it != g_tune_cache.end() &&
+        (it->second.path != 3 || askja::pair_supported(p->nc, p->dim, p->precision == ASKJA_FP64, p->n[p->dim - 1]))) {
       c->lc.force_rows = it->second.path;
       c->lc.rows_groups = it->second.groups;
       c->lc.small_occ = it->second.occupancy;
@@ -380,6 +430,39 @@ int askja_set_links(askja_ctx* c, const double* conf) {
   if (int rc = upload_conf(c, conf, cur_u(c))) return rc;
   CK(cudaMemcpyAsync(c->Uconf, cur_u(c), c->field_bytes, cudaMemcpyDeviceToDevice, c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  return ASKJA_OK;
+}
+
+int askja_set_links_async(askja_ctx* c, const double* conf) {
+  if (int rc = check_ctx(c)) return rc;
+  if (!conf) return set_err(c, ASKJA_ERR_ARG, "null buffer");
+  DevGuard g(c->p.device);
+  const size_t bytes = (size_t)c->nl * c->N * c->N * 2 * sizeof(double);
+  if (!c->copy_stream) {
+    CK(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+    for (int b = 0; b < 2; b++) {
+      CK(cudaMalloc(&c->up[b], bytes));
+      CK(cudaEventCreateWithFlags(&c->up_copied[b], cudaEventDisableTiming));
+      CK(cudaEventCreateWithFlags(&c->up_free[b], cudaEventDisableTiming));
+    }
+    CK(cudaMalloc(&c->up_bad, sizeof(unsigned long long)));
+    CK(cudaMemsetAsync(c->up_bad, 0, sizeof(unsigned long long), c->stream));
+  }
+  const int b = c->up_next;
+  c->up_next ^= 1;
+  // the copy waits for the conversion that last read this staging buffer (an
+  // event never recorded counts as complete), then overlaps whatever the
+  // engine's stream is running; the conversion is ordered after that work
+  CK(cudaStreamWaitEvent(c->copy_stream, c->up_free[b], 0));
+  CK(cudaMemcpyAsync(c->up[b], conf, bytes, cudaMemcpyHostToDevice, c->copy_stream));
+  CK(cudaEventRecord(c->up_copied[b], c->copy_stream));
+  CK(cudaStreamWaitEvent(c->stream, c->up_copied[b], 0));
+  askja::misc::k_count_nonfinite<<<4 * 148, 256, 0, c->stream>>>((const double*)c->up[b],
+                                                                  (long)(bytes / sizeof(double)), c->up_bad);
+  KL(cudaGetLastError(), "non-finite check");
+  KL(c->ks->from_conf(c->lc, c->up[b], cur_u(c)), "from_conf");
+  CK(cudaMemcpyAsync(c->Uconf, cur_u(c), c->field_bytes, cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaEventRecord(c->up_free[b], c->stream));
   return ASKJA_OK;
 }
 
@@ -644,10 +727,7 @@ int askja_leapfrog(askja_ctx* c, int nsteps, double eps) {
   if (int rc = check_ctx(c)) return rc;
   if (nsteps < 1) return set_err(c, ASKJA_ERR_ARG, "nsteps must be >= 1");
   DevGuard g(c->p.device);
-  for (int i = 0; i < nsteps; i++) {
-    KL(c->ks->force(c->lc, 1, cur_u(c), c->P, c->P, c->U[1 - c->cur], i == 0 ? 0.5 * eps : eps, eps), "kick+drift");
-    c->cur ^= 1;
-  }
+  if (int rc = fused_steps(c, nsteps, 0.5 * eps, eps)) return rc;
   KL(c->ks->force(c->lc, 0, cur_u(c), c->P, c->P, nullptr, 0.5 * eps, 0.0), "kick");
   CK(cudaStreamSynchronize(c->stream));
   return ASKJA_OK;
@@ -662,10 +742,7 @@ int askja_md_steps(askja_ctx* c, int nsteps, double eps) {
   KL(c->ks->drift(c->lc, cur_u(c), c->P2, eps), "drift");
   CK(cudaMemcpyAsync(c->P, c->P2, c->field_bytes, cudaMemcpyDeviceToDevice, c->stream));
   // ... then (K D) fused, in place on pi ...
-  for (int i = 1; i < nsteps; i++) {
-    KL(c->ks->force(c->lc, 1, cur_u(c), c->P, c->P, c->U[1 - c->cur], eps, eps), "kick+drift");
-    c->cur ^= 1;
-  }
+  if (int rc = fused_steps(c, nsteps - 1, eps, eps)) return rc;
   // ... and the last kick out of place: Pi = pi - eps F(u)
   KL(c->ks->force(c->lc, 0, cur_u(c), c->P, c->P2, nullptr, eps, 0.0), "kick");
   CK(cudaStreamSynchronize(c->stream));
@@ -681,6 +758,48 @@ int askja_trajectory(askja_ctx* c, int nsteps, askja_traj_result* out) {
   return read_state(c, out);
 }
 
+}  // extern "C"
+
+namespace {
+
+// Enqueue one trajectory, as a replay of the captured graph for this start
+// buffer and step count when use_graph (captured on first use).
+int launch_trajectory(askja_ctx* c, int nsteps, int use_graph) {
+  if (!use_graph) return enqueue_trajectory(c, nsteps);
+  const int start = c->cur;
+  if (!c->gexec[start] || c->g_nsteps[start] != nsteps) {
+    if (c->gexec[start]) cudaGraphExecDestroy(c->gexec[start]);
+    c->gexec[start] = nullptr;
+    cudaGraph_t graph;
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = enqueue_trajectory(c, nsteps);
+    cudaError_t ce = cudaStreamEndCapture(c->stream, &graph);
+    c->cur = start;
+    if (rc) return rc;
+    if (ce != cudaSuccess) return set_err(c, ASKJA_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+    ce = cudaGraphInstantiate(&c->gexec[start], graph, 0);
+    cudaGraphDestroy(graph);
+    if (ce != cudaSuccess) return set_err(c, ASKJA_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ce));
+    c->g_nsteps[start] = nsteps;
+  }
+  CK(cudaGraphLaunch(c->gexec[start], c->stream));
+  c->cur = start ^ (nsteps & 1);
+  return ASKJA_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int askja_trajectory_async(askja_ctx* c, int nsteps, askja_traj_result* out) {
+  if (int rc = check_ctx(c)) return rc;
+  if (nsteps < 1) return set_err(c, ASKJA_ERR_ARG, "nsteps must be >= 1");
+  DevGuard g(c->p.device);
+  if (int rc = launch_trajectory(c, nsteps, 1)) return rc;
+  if (out) CK(cudaMemcpyAsync(out, c->st, sizeof(TrajState), cudaMemcpyDeviceToHost, c->stream));
+  return ASKJA_OK;
+}
+
 int askja_run_trajectories(askja_ctx* c, int ntraj, int nsteps, int use_graph, askja_traj_result* last,
                            double* log) {
   if (int rc = check_ctx(c)) return rc;
@@ -689,30 +808,8 @@ int askja_run_trajectories(askja_ctx* c, int ntraj, int nsteps, int use_graph, a
   TrajState st0;
   CK(cudaMemcpyAsync(&st0, c->st, sizeof st0, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
-  for (int t = 0; t < ntraj; t++) {
-    if (!use_graph) {
-      if (int rc = enqueue_trajectory(c, nsteps)) return rc;
-      continue;
-    }
-    const int start = c->cur;
-    if (!c->gexec[start] || c->g_nsteps[start] != nsteps) {
-      if (c->gexec[start]) cudaGraphExecDestroy(c->gexec[start]);
-      c->gexec[start] = nullptr;
-      cudaGraph_t graph;
-      CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-      int rc = enqueue_trajectory(c, nsteps);
-      cudaError_t ce = cudaStreamEndCapture(c->stream, &graph);
-      c->cur = start;
-      if (rc) return rc;
-      if (ce != cudaSuccess) return set_err(c, ASKJA_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
-      ce = cudaGraphInstantiate(&c->gexec[start], graph, 0);
-      cudaGraphDestroy(graph);
-      if (ce != cudaSuccess) return set_err(c, ASKJA_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ce));
-      c->g_nsteps[start] = nsteps;
-    }
-    CK(cudaGraphLaunch(c->gexec[start], c->stream));
-    c->cur = start ^ (nsteps & 1);
-  }
+  for (int t = 0; t < ntraj; t++)
+    if (int rc = launch_trajectory(c, nsteps, use_graph)) return rc;
   CK(cudaStreamSynchronize(c->stream));
   if (int rc = read_state(c, last)) return rc;
   if (log && ntraj > 0) {
@@ -730,8 +827,9 @@ int askja_run_trajectories(askja_ctx* c, int ntraj, int nsteps, int use_graph, a
 
 int askja_set_tuning(askja_ctx* c, const askja_tuning* t) {
   if (int rc = check_ctx(c)) return rc;
-  if (!t || t->path < 0 || t->path > 2 || (t->path == 0 && c->N > 4) || t->groups < 0 ||
-      (t->path == 2 && !askja::tc_supported(c->N, c->D, c->p.precision == ASKJA_FP64)))
+  if (!t || t->path < 0 || t->path > 3 || (t->path == 0 && c->N > 4) || t->groups < 0 ||
+      (t->path == 2 && !askja::tc_supported(c->N, c->D, c->p.precision == ASKJA_FP64)) ||
+      (t->path == 3 && !askja::pair_supported(c->N, c->D, c->p.precision == ASKJA_FP64, c->lat.n[c->D - 1])))
     return set_err(c, ASKJA_ERR_ARG, "invalid tuning");
   c->lc.force_rows = t->path;
   c->lc.rows_groups = t->groups;
@@ -755,6 +853,10 @@ int askja_autotune(askja_ctx* c, int reps, askja_tuning* out) {
     cands.push_back({0, 0, 2});
   }
   if (askja::tc_supported(c->N, c->D, fp64)) cands.push_back({2, 0, 0});
+  if (askja::pair_supported(c->N, c->D, fp64, c->lat.n[c->D - 1])) {
+    cands.push_back({3, 0, 0});
+    cands.push_back({3, 0, 1});
+  }
   std::vector<int> seen;
   for (int want : {0, 2, 4, 8, 16, 32, 64}) {
     const int eff = askja::rows_effective_groups(c->N, fp64, want);
@@ -779,11 +881,19 @@ int askja_autotune(askja_ctx* c, int reps, askja_tuning* out) {
     lc.force_rows = cands[i].path;
     lc.rows_groups = cands[i].groups;
     lc.small_occ = cands[i].occ;
-    cudaError_t e = c->ks->force(lc, 1, cur_u(c), c->P2, c->P2, c->U[1 - c->cur], 0.5 * c->p.dt, c->p.dt);
+    // the site-pair candidate runs on the site-pair layout (swapped back below)
+    const bool pl = cands[i].path == 3;
+    cudaError_t e = cudaSuccess;
+    if (pl) e = c->ks->pair_swap(lc, cur_u(c));
+    if (pl && e == cudaSuccess) e = c->ks->pair_swap(lc, c->P2);
+    if (e == cudaSuccess)
+      e = c->ks->force(lc, 1, cur_u(c), c->P2, c->P2, c->U[1 - c->cur], 0.5 * c->p.dt, c->p.dt);
     if (e == cudaSuccess) e = cudaEventRecord(e0, c->stream);
     for (int r = 0; r < reps && e == cudaSuccess; r++)
       e = c->ks->force(lc, 1, cur_u(c), c->P2, c->P2, c->U[1 - c->cur], 0.5 * c->p.dt, c->p.dt);
     if (e == cudaSuccess) e = cudaEventRecord(e1, c->stream);
+    if (pl && e == cudaSuccess) e = c->ks->pair_swap(lc, cur_u(c));
+    if (pl && e == cudaSuccess) e = c->ks->pair_swap(lc, c->P2);
     if (e == cudaSuccess) e = cudaEventSynchronize(e1);
     float ms = 0.f;
     if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);

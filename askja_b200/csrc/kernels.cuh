@@ -8,6 +8,7 @@
 #include "misc.cuh"
 #include "rows.cuh"
 #include "small.cuh"
+#include "pair.cuh"
 #include "eig.cuh"
 #include "tc.cuh"
 
@@ -179,13 +180,41 @@ cudaError_t tc_dispatch(const LaunchCtx& c, int mode, const void* U, const void*
   return cudaErrorInvalidValue;
 }
 
+// Fused kick+drift on site pairs (FP32 SU(3)); U, P and Uout in the site-pair
+// layout, P updated in place.
+template <typename T>
+cudaError_t pair_force(const LaunchCtx& c, const void* U, const void* Pin, void* Pout, void* Uout, double ek,
+                       double ed) {
+  if constexpr (sizeof(T) == 4) {
+    if (Pin != Pout || !pair_supported(c.lat.N, c.lat.D, false, c.lat.n[c.lat.D - 1])) return cudaErrorInvalidValue;
+    const unsigned grid = blocks_for(c.lat.V, 64);
+    const int threads = 32 * std::min(c.lat.D, 4);
+    auto k = c.small_occ ? pair::k_force_pair<1> : pair::k_force_pair<0>;
+    k<<<grid, threads, 0, c.stream>>>(c.lat, (const float2*)U, (float2*)Pout, (float2*)Uout, (float)ek, (float)ed,
+                                      c.order, c.reunit);
+    return cudaGetLastError();
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <typename T>
+cudaError_t pair_swap(const LaunchCtx& c, void* f) {
+  if constexpr (sizeof(T) == 4) {
+    const long n4 = (long)(field_elems(c.lat) / 2);
+    pair::k_pair_swap<<<(unsigned)std::min<long>(blocks_for(n4, 256), 148L * 16), 256, 0, c.stream>>>((float4*)f, n4);
+    return cudaGetLastError();
+  }
+  return cudaErrorInvalidValue;
+}
+
 template <typename T>
 cudaError_t force(const LaunchCtx& c, int mode, const void* U, const void* Pin, void* Pout, void* Uout, double ek,
                   double ed) {
   const int N = c.lat.N;
   if (c.force_rows == 2 && tc_supported(N, c.lat.D, sizeof(T) == 8))
     return tc_dispatch<T>(c, mode, U, Pin, Pout, Uout, ek, ed);
-  if (!c.force_rows) {
+  if (c.force_rows == 3 && mode == 1) return pair_force<T>(c, U, Pin, Pout, Uout, ek, ed);
+  if (!c.force_rows || c.force_rows == 3) {
     if (N == 2) return small_force<2, T>(c, mode, U, Pin, Pout, Uout, ek, ed);
     if (N == 3) return small_force<3, T>(c, mode, U, Pin, Pout, Uout, ek, ed);
     if (N == 4) return small_force<4, T>(c, mode, U, Pin, Pout, Uout, ek, ed);
@@ -202,7 +231,7 @@ cudaError_t drift(const LaunchCtx& c, void* U, const void* P, double eps) {
   const int N = c.lat.N;
   if (c.force_rows == 2 && tc_supported(N, c.lat.D, sizeof(T) == 8))
     return tc_dispatch<T>(c, 2, U, P, nullptr, U, 0.0, eps);
-  if (!c.force_rows) {
+  if (!c.force_rows || c.force_rows == 3) {
     if (N == 2) return small_drift<2, T>(c, U, P, eps);
     if (N == 3) return small_drift<3, T>(c, U, P, eps);
     if (N == 4) return small_drift<4, T>(c, U, P, eps);
@@ -219,7 +248,7 @@ cudaError_t reunit(const LaunchCtx& c, void* U) {
   using S2 = typename Storage<T>::type;
   const int N = c.lat.N;
   const unsigned gsm = blocks_for(nlinks(c.lat), SMALL_THREADS);
-  if (!c.force_rows) {
+  if (!c.force_rows || c.force_rows == 3) {
     if (N == 2) {
       small::k_reunit<2, T, S2><<<gsm, SMALL_THREADS, 0, c.stream>>>(c.lat, (S2*)U);
       return cudaGetLastError();
@@ -389,7 +418,7 @@ cudaError_t to_conf(const LaunchCtx& c, const void* f, void* conf) {
 template <typename T>
 constexpr KernelSet make_set() {
   return KernelSet{&force<T>,   &drift<T>,   &reunit<T>,  &plaq<T>,           &linksums<T>,  &gauss<T>, &lines<T>,
-                   &slice_trace<T>, &line_eigs<T>, &refresh<T>, &identity<T>, &gauss_matrices<T>, &from_conf<T>, &to_conf<T>};
+                   &slice_trace<T>, &line_eigs<T>, &refresh<T>, &identity<T>, &gauss_matrices<T>, &from_conf<T>, &to_conf<T>, &pair_swap<T>};
 }
 
 }  // namespace detail

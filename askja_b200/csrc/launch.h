@@ -16,7 +16,9 @@ struct LaunchCtx {
   int order;        // effective Taylor order
   int reunit;       // reunitarise after each link update
   int force_rows;   // kernel mapping: 0 thread-per-link (NC <= 4), 1 row-per-thread,
-                    // 2 tensor cores (FP32, NC = 32 or 64, DIM >= 2)
+                    // 2 tensor cores (FP32, NC = 32 or 64, DIM >= 2), 3 site pairs in
+                    // packed FP32 (NC = 3, even n[DIM-1]; the fused kick+drift then
+                    // expects the site-pair layout, see pair_swap)
   int rows_groups;  // row kernels: sites per CTA (0: default 128/NC)
   int small_occ;    // thread-per-link kernels: register budget for 0 default, 1 / 2 more resident CTAs
   void* scratch;    // tensor-core path: per-link contiguous copy of U (V*D*NC*NC float2)
@@ -28,6 +30,11 @@ struct LaunchCtx {
 
 // whether the tensor-core mapping exists for this shape and precision
 inline bool tc_supported(int N, int D, bool fp64) { return !fp64 && (N == 32 || N == 64) && D >= 2; }
+
+// whether the site-pair mapping exists (n_fast: extent of the fastest direction)
+inline bool pair_supported(int N, int D, bool fp64, int n_fast) {
+  return !fp64 && N == 3 && D >= 2 && n_fast % 2 == 0;
+}
 
 // Scalar reductions return their values in device memory:
 //   plaq     -> out[0] temporal, out[1] spatial
@@ -54,6 +61,8 @@ struct KernelSet {
   cudaError_t (*gauss_matrices)(const LaunchCtx&, void* U, uint64_t seed);
   cudaError_t (*from_conf)(const LaunchCtx&, const void* conf, void* f);
   cudaError_t (*to_conf)(const LaunchCtx&, const void* f, void* conf);
+  // canonical <-> site-pair layout of a field, in place (FP32 only)
+  cudaError_t (*pair_swap)(const LaunchCtx&, void* f);
 };
 
 // size (in doubles) of the partial buffer the reductions need

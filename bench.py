@@ -229,16 +229,22 @@ class _Null:
 
 
 def time_fused_kernel(e, stream_ptr, device, nlaunch, dt):
-    """Average duration of the fused kick+drift kernel: nlaunch back-to-back
-    launches (askja_leapfrog issues nlaunch fused launches + 1 kick)."""
+    """Average duration of one fused kick+drift launch: the slope between
+    askja_leapfrog runs of nlaunch and 2 nlaunch fused launches, so that the
+    closing kick and the layout conversions around the loop (site-pair
+    mapping) cancel."""
+    import torch
     s, t0, t1 = event_timer(stream_ptr, device)
+    t2 = torch.cuda.Event(enable_timing=True)
     e.leapfrog(2, dt)
     e.sync()
     t0.record(s)
     e.leapfrog(nlaunch, dt)
     t1.record(s)
-    t1.synchronize()
-    return t0.elapsed_time(t1) / (nlaunch + 1)
+    e.leapfrog(2 * nlaunch, dt)
+    t2.record(s)
+    t2.synchronize()
+    return (t1.elapsed_time(t2) - t0.elapsed_time(t1)) / nlaunch
 
 
 def run_ours(args):
@@ -277,7 +283,7 @@ def run_ours(args):
                 # dominant kernel: fused kick+drift, timed alone
                 r["kernel_ms"] = time_fused_kernel(e, e.stream_ptr, dev, 20, cfg["dt"])
                 # e2e through the C ABI with host buffers
-                r.update(run_e2e(e, nsteps, max(3, K // 2), world))
+                r.update(run_e2e(e, nsteps, max(6, K), world))
                 t, s_ = e.PlaqExp()
                 r["plaq"] = 1.0 - (t + s_) / (vol * 6)
             res[prec] = r
@@ -313,10 +319,24 @@ def run_ours(args):
                     "flops_per_launch": fpl * links, "avg_launch_ms": f32["kernel_ms"],
                     "hbm_achieved_gbs": achieved}
     else:
-        roofline = {"bound": "hbm", "kernel": f"fused kick+drift (small::k_force<{nc},float,1>)",
+        paired = f32["tuning"]["path"] == 3
+        kname = "pair::k_force_pair (site pairs, packed FP32x2)" if paired else f"small::k_force<{nc},float,1>"
+        # the FP32 floor beside the HBM one: complex products per link = 4(D-1) + 1 force
+        # products + X^2 and E U of the Cayley-Hamilton exponential (N <= 3; LEVEL Horner
+        # products otherwise), 8 NC^3 flops each, against the FFMA peak measured now
+        order = cfg["level"] if 0 <= cfg["level"] <= 8 else 8
+        fpl = 8 * nc ** 3 * (4 * (len(dims) - 1) + 1 + (2 if nc <= 3 else order))
+        pk32 = fp32_peak(dev)
+        tf32 = fpl * links / (f32["kernel_ms"] / 1e3) / 1e12
+        roofline = {"bound": "hbm", "kernel": f"fused kick+drift ({kname})",
                     "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                    "peak_source": peak_kind, "traffic": traffic,
-                    "bytes_per_launch": bytes_per_lu * links, "avg_launch_ms": f32["kernel_ms"]}
+                    "peak_source": peak_kind, "traffic": None if paired else traffic,
+                    "bytes_per_launch": bytes_per_lu * links, "avg_launch_ms": f32["kernel_ms"],
+                    "fp32": {"flops_per_launch": fpl * links, "achieved": tf32, "peak": pk32, "unit": "TFLOP/s",
+                             "frac": tf32 / pk32,
+                             "peak_source": "measured FFMA on this device (askja_peak_flops)",
+                             "note": "matrix-product flops only (Cayley-Hamilton scalars, projection, "
+                                     "reunitarisation not counted)"}}
     field_mb = links * nc * nc * 8 / 1e6
     line = {
         "metric": f"link-updates/s (1 B200): FP32-mixed HMC trajectories, SU({nc}) {'x'.join(map(str, dims))}",
@@ -346,7 +366,9 @@ def run_ours(args):
         "mean_abs_dH": f32["dh_abs"],
         "plaquette": f32["plaq"],
         "e2e": {"value": f32["e2e_lu"], "unit": "link-updates/s", "h2d_bytes_per_step": f32["h2d"],
-                "d2h_bytes_per_step": f32["d2h"]},
+                "d2h_bytes_per_step": f32["d2h"], "steps": f32["e2e_K"],
+                "api": "askja_set_links_async (FP64 U-conf from pinned host memory) + askja_trajectory_async "
+                       "(outcome to pinned host memory) per trajectory; uploads overlap the previous trajectory"},
         "roofline": roofline,
         "gpu_launches": f32["K"] * (nsteps + 15) + f64["K"] * (nsteps + 15),
         "clocks": f32["clocks"],
@@ -388,27 +410,46 @@ def measured_traffic(config: str):
 
 
 def run_e2e(e, nsteps, K, world):
-    """Same metric through the C ABI with host buffers: per trajectory, upload
-    the configuration from pinned host memory (FP64 U-conf layout) and read
-    the trajectory result back."""
+    """Same metric through the C ABI with host buffers.  Every trajectory's
+    starting configuration (FP64 U-conf layout, the reference's interchange
+    format) is uploaded from pinned host memory with askja_set_links_async
+    (two host buffers used in turn) and its outcome (askja_traj_result) read
+    back to pinned host memory with askja_trajectory_async, so the upload for
+    trajectory k+1 runs on the copy engine while trajectory k computes.  Timed
+    on the host from the first upload to the synchronisation after the last
+    read-back."""
+    import ctypes
+
     import askja_b200 as ab
     nbytes = int(np.prod(e.shape)) * 16
-    buf = ab.PinnedBuffer.alloc(nbytes)
+    rsz = ctypes.sizeof(ab.TrajResult)
+    bufs = [ab.PinnedBuffer.alloc(nbytes) for _ in range(2)]
+    res = ab.PinnedBuffer.alloc(rsz * (K + 1))
     try:
-        host = buf.array(np.complex128, e.shape)
-        host[...] = e.get_links()
-        e.trajectory(nsteps)  # warm (graphs not used on this path)
+        u = e.get_links()
+        for b in bufs:
+            b.array(np.complex128, e.shape)[...] = u
+        # untimed: staging buffers, graph capture
+        e.set_links_async(bufs[0].ptr)
+        e.trajectory_async(nsteps, res.ptr + K * rsz)
+        e.sync()
         barrier(world)
         t0 = time.perf_counter()
-        for _ in range(K):
-            e.set_links_ptr(buf.ptr)
-            e.trajectory(nsteps)
+        for k in range(K):
+            e.set_links_async(bufs[k % 2].ptr)
+            e.trajectory_async(nsteps, res.ptr + k * rsz)
+        e.sync()
         dt = time.perf_counter() - t0
+        outs = [ab.TrajResult.from_address(res.ptr + k * rsz).as_dict() for k in range(K)]
+        assert all(np.isfinite(o["dh"]) for o in outs)
+        assert [o["n_tot"] for o in outs] == sorted(o["n_tot"] for o in outs)
     finally:
-        buf.free()
+        for b in bufs:
+            b.free()
+        res.free()
     dt = max_over_ranks(dt, world)
     links = e.vol * e.dim
-    return {"e2e_lu": aggregate_rate(links * nsteps * K, world, dt), "h2d": nbytes, "d2h": 72}
+    return {"e2e_lu": aggregate_rate(links * nsteps * K, world, dt), "h2d": nbytes, "d2h": rsz, "e2e_K": K}
 
 
 def cpu_baseline(cfg, md_steps):
@@ -578,9 +619,10 @@ def run_reference(args):
 def run_kernel_only(args):
     """Kernel microbenchmark (also the command the ncu summaries under
     profiles/ capture): one engine of the config, Haar hot start, Philox
-    momenta, then `--steps` fused kick+drift launches (askja_leapfrog: steps
-    fused launches + 1 kick) with the default (untuned) kernel mapping or the
-    one `--path` forces.  Prints the average launch time."""
+    momenta, `--warmup` single-step leapfrogs, then askja_leapfrog runs of 2,
+    `--steps` and 2 `--steps` fused kick+drift launches (each + 1 kick) with
+    the default (untuned) kernel mapping or the one `--path` forces.  Prints
+    the launch time from the slope between the last two runs."""
     import torch
 
     import askja_b200 as ab
@@ -588,19 +630,16 @@ def run_kernel_only(args):
     nc, dims = cfg["nc"], cfg["dims"]
     with ab.Engine(nc, dims, beta=cfg["beta"], dt=cfg["dt"], level=cfg["level"], precision=args.precision,
                    kernel_path=args.path) as e:
+        if args.occ:
+            ab.set_tuning(e, {"path": args.path, "occupancy": args.occ})
         e.hot_start(11)
         e.initializeE(11, 0)
         for _ in range(args.warmup):
             e.leapfrog(1, cfg["dt"])
         e.sync()
-        s, t0, t1 = event_timer(e.stream_ptr, 0)
-        t0.record(s)
-        e.leapfrog(args.steps, cfg["dt"])
-        t1.record(s)
-        t1.synchronize()
-        ms = t0.elapsed_time(t1) / (args.steps + 1)
-    return {"kernel_only": args.config, "precision": args.precision, "path": args.path,
-            "launches": args.steps + 1, "avg_launch_ms": ms,
+        ms = time_fused_kernel(e, e.stream_ptr, 0, args.steps, cfg["dt"])
+    return {"kernel_only": args.config, "precision": args.precision, "path": args.path, "occ": args.occ,
+            "launches": 3 * args.steps + 2, "avg_launch_ms": ms,
             "link_updates_per_s": int(np.prod(dims)) * len(dims) / (ms / 1e3)}
 
 
@@ -618,6 +657,7 @@ def main():
     ap.add_argument("--no-tune", action="store_true", help="default kernel mapping, no autotuning")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"], help="with --kernel-only")
     ap.add_argument("--path", type=int, default=0, help="with --kernel-only: askja kernel_path")
+    ap.add_argument("--occ", type=int, default=0, help="with --kernel-only: register budget (askja_tuning.occupancy)")
     args = ap.parse_args()
     if args.kernel_only:
         line = run_kernel_only(args)

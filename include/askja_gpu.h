@@ -66,7 +66,9 @@ typedef struct {
   int reunitarise;     /* -1 default (on for FP32, off for FP64), 0 off, 1 on */
   int device;          /* CUDA device ordinal */
   int kernel_path;     /* 0 automatic; 1 row-per-thread kernels for every NC (testing);
-                          2 tensor cores (FP32 with NC = 32 or 64 and DIM >= 2 only) */
+                          2 tensor cores (FP32 with NC = 32 or 64 and DIM >= 2 only);
+                          3 site pairs in packed FP32 (NC = 3, FP32, DIM >= 2 and
+                            an even extent N{DIM-1} only) */
   uint64_t seed;       /* Philox key for momenta, Metropolis uniforms and hot start */
 } askja_params;
 
@@ -99,6 +101,17 @@ ASKJA_API int askja_sync(askja_ctx* ctx);
 /* u := conf and uconf := conf (loadconf + takeconfiguration, sun.cpp:744-765,
  * 1164-1170).  Rejects non-finite input with ASKJA_ERR_NONFINITE. */
 ASKJA_API int askja_set_links(askja_ctx* ctx, const double* conf);
+/* The same upload without blocking the host (not in the reference): the
+ * host->device copy runs on a copy stream into one of two device staging
+ * buffers (used in turn), overlapping the work already enqueued on the
+ * context's stream; the conversion into u and uconf is ordered after that
+ * work, so a trajectory enqueued next starts from conf.  Returns once the
+ * copy is enqueued.  conf should be page-locked (askja_host_alloc) and must
+ * stay unchanged until a synchronising call (askja_sync, askja_trajectory,
+ * a getter) has returned.  Non-finite input is counted on the device and
+ * reported as ASKJA_ERR_NONFINITE by the next synchronising call (u then
+ * holds the converted values). */
+ASKJA_API int askja_set_links_async(askja_ctx* ctx, const double* conf);
 ASKJA_API int askja_get_links(askja_ctx* ctx, double* conf);          /* current u */
 ASKJA_API int askja_get_saved_links(askja_ctx* ctx, double* conf);    /* uconf (what storeconf writes, sun.cpp:289-302) */
 /* which = 0: pi (current momenta), 1: Pi (updated momenta) */
@@ -146,6 +159,12 @@ ASKJA_API int askja_eigenphases(askja_ctx* ctx, double* w, double* p);
  * kick halved, H_new, Metropolis, then uconf = u (accept) or u = uconf
  * (reject).  No host synchronisation inside. */
 ASKJA_API int askja_trajectory(askja_ctx* ctx, int nsteps, askja_traj_result* out);
+/* askja_trajectory without waiting (not in the reference): enqueues the
+ * trajectory (a CUDA-graph replay, as askja_run_trajectories) and the copy of
+ * its outcome to *out (may be NULL), and returns.  *out is valid after the
+ * next askja_sync; it should be page-locked, or the copy blocks the host
+ * until the trajectory has run. */
+ASKJA_API int askja_trajectory_async(askja_ctx* ctx, int nsteps, askja_traj_result* out);
 /* `ntraj` trajectories; with use_graph != 0 each is a CUDA-graph replay.
  * `log` (may be NULL) receives 4 doubles per trajectory: h_old, h_new, dh, accepted. */
 ASKJA_API int askja_run_trajectories(askja_ctx* ctx, int ntraj, int nsteps, int use_graph, askja_traj_result* last,
@@ -165,11 +184,12 @@ ASKJA_API int askja_md_steps(askja_ctx* ctx, int nsteps, double eps);
 /* Kernel mapping for the force / link-update kernel of one (NC, DIM,
  * precision): thread-per-link (NC <= 4, all matrices in registers) or
  * row-per-thread (NC threads per link, shared-memory tiles) or tensor cores
- * (FP32, NC = 32 or 64: every complex product a split-TF32 MMA), the number
- * of sites per CTA of the row kernels, and the register budget of the
- * thread-per-link kernels. */
+ * (FP32, NC = 32 or 64: every complex product a split-TF32 MMA) or site pairs
+ * (FP32 SU(3): two adjacent sites' links per thread in packed FP32x2
+ * arithmetic), the number of sites per CTA of the row kernels, and the
+ * register budget of the thread-per-link kernels. */
 typedef struct {
-  int path;       /* 0 thread-per-link, 1 row-per-thread, 2 tensor cores */
+  int path;       /* 0 thread-per-link, 1 row-per-thread, 2 tensor cores, 3 site pairs */
   int groups;     /* row-per-thread: sites per CTA (0 = default) */
   int occupancy;  /* thread-per-link: 0 default registers, 1 and 2 tighter budgets / more resident CTAs */
   int ncand;      /* candidates timed */
