@@ -312,11 +312,105 @@ __device__ __forceinline__ void expi_times_ch(Mat<N, T>& Tm, const Mat<N, T>& P,
   mul_nn(Tm, E, Ux);
 }
 
-// Link update of the FP32 path: the Cayley-Hamilton form where it exists;
-// the FP64 path keeps the reference's Horner evaluation.
+// The same series for N = 3 written in P, for Hermitian P (every momentum
+// field of the reference and of this engine: the refresh draws P in the
+// algebra and the kick adds the same real part to P_ij and P_ji and opposite
+// imaginary parts, so P_ij = conj(P_ji) holds exactly; the diagonal is taken
+// real).  With X = i eps P, tr X = i tau, det X = i d and the coefficient c1
+// of the characteristic polynomial are imaginary, imaginary and real, so the
+// coefficients of X^k = al_k 1 + be_k X + ga_k X^2 are al_k = i^k a_k,
+// be_k = i^(k-1) b_k, ga_k = i^(k-2) g_k with a real recursion
+//   a_k = -d g_(k-1),  b_k = a_(k-1) + c1 g_(k-1),  g_k = b_(k-1) + tau g_(k-1),
+// and  E = A 1 + B P + C P^2  with  A = sum i^k a_k/k!, B = eps sum i^k b_k/k!,
+// C = eps^2 sum i^k g_k/k!.  P^2 is Hermitian: its upper triangle and real
+// diagonal are formed (no X, no full X^2 product).
+template <typename T>
+__device__ __forceinline__ void expi_times_herm3(Mat<3, T>& Tm, const Mat<3, T>& P, const Mat<3, T>& Ux, T eps,
+                                                 int order) {
+  const T p0 = P.a[0][0].re, p1 = P.a[1][1].re, p2 = P.a[2][2].re;
+  const cpx<T>& P01 = P.a[0][1];
+  const cpx<T>& P02 = P.a[0][2];
+  const cpx<T>& P12 = P.a[1][2];
+  const T n01 = cnorm2_add(P01, T(0)), n02 = cnorm2_add(P02, T(0)), n12 = cnorm2_add(P12, T(0));
+  // Q = P^2: diagonal and upper triangle
+  const T q0 = fma(p0, p0, n01 + n02), q1 = fma(p1, p1, n01 + n12), q2 = fma(p2, p2, n02 + n12);
+  const T s01 = p0 + p1, s02 = p0 + p2, s12 = p1 + p2;
+  cpx<T> Q01 = mkc<T>(s01 * P01.re, s01 * P01.im);
+  cmac_nc(Q01, P02, P12);  // + P02 P21
+  cpx<T> Q02 = mkc<T>(s02 * P02.re, s02 * P02.im);
+  cmac(Q02, P01, P12);  // + P01 P12
+  cpx<T> Q12 = mkc<T>(s12 * P12.re, s12 * P12.im);
+  cmac_cn(Q12, P01, P02);  // + P10 P02
+  // invariants: tr P, tr P^2, det P (real)
+  const T trp = p0 + p1 + p2;
+  const T trq = q0 + q1 + q2;
+  const cpx<T> t = cmul(P01, P12);
+  const T re3 = fma(t.re, P02.re, t.im * P02.im);  // Re(P01 P12 P20)
+  T det = p0 * fma(p1, p2, -n12);
+  det = fma(-p1, n02, det);
+  det = fma(-p2, n01, det);
+  det = fma(T(2), re3, det);
+  const T tau = eps * trp;
+  const T c1 = T(0.5) * fma(eps * eps, trq, -tau * tau);
+  const T d = -(eps * eps * eps) * det;
+  T a = T(1), b = T(0), g = T(0);
+  cpx<T> A = mkc<T>(T(1), T(0)), B = czero<T>(), C = czero<T>();
+  T f = T(1);
+#pragma unroll
+  for (int k = 1; k <= 8; k++) {  // order <= 8; unrolled so that 1/k! and i^k are constants
+    if (k > order) break;
+    const T na = -d * g;
+    const T nb = fma(c1, g, a);
+    const T ng = fma(tau, g, b);
+    a = na;
+    b = nb;
+    g = ng;
+    f = f * T(1.0 / k);
+    const T sf = (k & 2) ? -f : f;  // i^k = +1, +i, -1, -i
+    if (k & 1) {
+      A.im = fma(sf, a, A.im);
+      B.im = fma(sf, b, B.im);
+      C.im = fma(sf, g, C.im);
+    } else {
+      A.re = fma(sf, a, A.re);
+      B.re = fma(sf, b, B.re);
+      C.re = fma(sf, g, C.re);
+    }
+  }
+  B.re *= eps;
+  B.im *= eps;
+  const T e2 = eps * eps;
+  C.re *= e2;
+  C.im *= e2;
+  Mat<3, T> E;
+  const T pd[3] = {p0, p1, p2}, qd[3] = {q0, q1, q2};
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    E.a[i][i].re = fma(C.re, qd[i], fma(B.re, pd[i], A.re));
+    E.a[i][i].im = fma(C.im, qd[i], fma(B.im, pd[i], A.im));
+  }
+  const cpx<T> Qu[3] = {Q01, Q02, Q12};
+  const int iu[3] = {0, 0, 1}, ju[3] = {1, 2, 2};
+#pragma unroll
+  for (int u = 0; u < 3; u++) {
+    const int i = iu[u], j = ju[u];
+    cpx<T> e = cmul(B, P.a[i][j]);  // upper: B P_ij + C Q_ij
+    cmac(e, C, Qu[u]);
+    E.a[i][j] = e;
+    cpx<T> l = cmul(B, P.a[j][i]);  // lower: B P_ji + C conj(Q_ij)
+    cmac_nc(l, C, Qu[u]);
+    E.a[j][i] = l;
+  }
+  mul_nn(Tm, E, Ux);
+}
+
+// Link update of the FP32 path: the Cayley-Hamilton form (for N = 3 in P,
+// Hermitian P); the FP64 path keeps the reference's Horner evaluation.
 template <int N, typename T>
 __device__ __forceinline__ void expi_update(Mat<N, T>& Tm, const Mat<N, T>& P, const Mat<N, T>& Ux, T eps, int order) {
-  if constexpr (sizeof(T) == 4 && N <= 3)
+  if constexpr (sizeof(T) == 4 && N == 3)
+    expi_times_herm3(Tm, P, Ux, eps, order);
+  else if constexpr (sizeof(T) == 4 && N == 2)
     expi_times_ch(Tm, P, Ux, eps, order);
   else
     expi_times(Tm, P, Ux, eps, order);
@@ -340,7 +434,11 @@ __device__ __forceinline__ void reunitarise(Mat<N, T>& M) {
     T nrm = T(0);
 #pragma unroll
     for (int k = 0; k < N; k++) nrm = cnorm2_add(M.a[r][k], nrm);
-    const T inv = T(1) / sqrt(nrm);
+    T inv;
+    if constexpr (sizeof(T) == 4)
+      inv = rsqrtf(nrm);  // FP32 path: the approximate reciprocal square root (2 ulp) suffices
+    else
+      inv = T(1) / sqrt(nrm);
 #pragma unroll
     for (int k = 0; k < N; k++) {
       M.a[r][k].re *= inv;
