@@ -116,8 +116,8 @@ ASKJA_API int askja_get_links(askja_ctx* ctx, double* conf);          /* current
 ASKJA_API int askja_get_saved_links(askja_ctx* ctx, double* conf);    /* uconf (what storeconf writes, sun.cpp:289-302) */
 /* which = 0: pi (current momenta), 1: Pi (updated momenta).  Momenta are
  * Hermitian (P_ij = conj(P_ji), real diagonal) as the reference's are; the
- * ASKJA_FP32 SU(3) link update relies on it (it forms exp(i eps P) from the
- * diagonal and upper triangle of P). */
+ * ASKJA_FP32 SU(3) link update relies on it (P^2, tr P and det P are formed
+ * from the real diagonal and the upper triangle). */
 ASKJA_API int askja_set_momenta(askja_ctx* ctx, int which, const double* conf);
 ASKJA_API int askja_get_momenta(askja_ctx* ctx, int which, double* conf);
 ASKJA_API int askja_initializeU(askja_ctx* ctx);                       /* cold start, sun.cpp:194-207; also uconf */
