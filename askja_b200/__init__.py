@@ -45,6 +45,7 @@ EXPORTS = [
     "askja_batch_create", "askja_batch_destroy", "askja_batch_last_error", "askja_batch_stream",
     "askja_batch_hot_start", "askja_batch_set_links", "askja_batch_get_links", "askja_batch_run",
     "askja_batch_plaquette", "askja_autotune", "askja_set_tuning", "askja_set_links_async", "askja_trajectory_async",
+    "askja_FourierTrafo", "askja_Tab", "askja_Tab_all",
 ]
 
 
@@ -123,6 +124,9 @@ def library() -> ctypes.CDLL:
     L.askja_WilsonLoopDir.argtypes = [vp, ip, dp]
     L.askja_PlaqExp.argtypes = [vp, dp, dp]
     L.askja_eigenphases.argtypes = [vp, dp, dp]
+    L.askja_FourierTrafo.argtypes = [vp, dp]
+    L.askja_Tab.argtypes = [vp, ctypes.c_long, dp, ip]
+    L.askja_Tab_all.argtypes = [vp, ip, dp]
     L.askja_trajectory.argtypes = [vp, ip, ctypes.POINTER(TrajResult)]
     L.askja_trajectory_async.argtypes = [vp, ip, vp]
     L.askja_run_trajectories.argtypes = [vp, ip, ip, ip, ctypes.POINTER(TrajResult), dp]
@@ -317,6 +321,24 @@ class Engine:
     def scalarLoopcorr(self):
         out = np.zeros(self.dims[0])
         self._ck(self.lib.askja_scalarLoopcorr(self._ctx, _dptr(out)))
+        return out
+
+    def FourierTrafo(self):
+        """askja_FourierTrafo: |inverse DFT| of the plaquette energy of sites 0..N0-1."""
+        out = np.zeros(self.dims[0])
+        self._ck(self.lib.askja_FourierTrafo(self._ctx, _dptr(out)))
+        return out
+
+    def Tab(self, site: int, npt: int, mdata=None):
+        """askja_Tab: add site's energy-momentum tensor terms to mdata (zeros if None)."""
+        m = np.zeros(npt) if mdata is None else np.ascontiguousarray(mdata, dtype=np.float64)
+        self._ck(self.lib.askja_Tab(self._ctx, int(site), _dptr(m), int(npt)))
+        return m
+
+    def Tab_all(self, npt: int):
+        """askja_Tab_all: per-site contributions, shape (V, npt)."""
+        out = np.zeros((self.vol, npt))
+        self._ck(self.lib.askja_Tab_all(self._ctx, int(npt), _dptr(out)))
         return out
 
     def hamiltonian(self, which: int = 0):

@@ -32,7 +32,7 @@ NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xco
                   "--expt-relaxed-constexpr", "-ccbin", CXX]
 CU_SOURCES = ["kernels_fp64.cu", "kernels_fp32.cu", "engine.cu", "static_plaq.cu", "peak.cu", "batch.cu"]
 CPP_SOURCES = ["hostio.cpp"]
-HEADERS = ["common.cuh", "small.cuh", "rows.cuh", "misc.cuh", "kernels.cuh", "launch.h", "batch.cuh", "tc.cuh", "eig.cuh", "pair.cuh"]
+HEADERS = ["common.cuh", "small.cuh", "rows.cuh", "misc.cuh", "kernels.cuh", "launch.h", "batch.cuh", "tc.cuh", "eig.cuh", "pair.cuh", "tab.cuh"]
 
 
 def _newer(target: str, deps) -> bool:

@@ -723,6 +723,47 @@ int askja_scalarLoopcorr(askja_ctx* c, double* out) {
   return scal(c, c->lines, out, c->lat.n[0]);
 }
 
+int askja_FourierTrafo(askja_ctx* c, double* coefficients) {
+  if (int rc = check_ctx(c)) return rc;
+  if (!coefficients) return set_err(c, ASKJA_ERR_ARG, "null output");
+  if (c->N > 64) return set_err(c, ASKJA_ERR_ARG, "FourierTrafo: NC <= 64");
+  DevGuard g(c->p.device);
+  const int n = c->lat.n[0];
+  KL(c->ks->fourier(c->lc, cur_u(c), n, c->partial, c->lines), "FourierTrafo");
+  return scal(c, c->lines, coefficients, n);
+}
+
+// Tab of sites [site0, site0 + nsites) into the device buffer out (k*npt + m)
+static int tab_range(askja_ctx* c, long site0, long nsites, int npt, double* out_dev) {
+  if (c->D > 8 || c->N > 64) return set_err(c, ASKJA_ERR_ARG, "Tab: DIM <= 8 and NC <= 64");
+  if (npt < 2 || npt > c->D + 2) return set_err(c, ASKJA_ERR_ARG, "Tab: Npt must be in 2..DIM+2 (got %d)", npt);
+  KL(c->ks->tab(c->lc, cur_u(c), c->P, c->P2, (int)site0, (int)nsites, npt, out_dev), "Tab");
+  return ASKJA_OK;
+}
+
+int askja_Tab(askja_ctx* c, long site, double* mdata, int npt) {
+  if (int rc = check_ctx(c)) return rc;
+  if (!mdata) return set_err(c, ASKJA_ERR_ARG, "null output");
+  if (site < 0 || site >= c->V) return set_err(c, ASKJA_ERR_ARG, "site %ld outside 0..%ld", site, c->V - 1);
+  DevGuard g(c->p.device);
+  if (int rc = tab_range(c, site, 1, npt, c->partial)) return rc;  // partial: >= 64 doubles
+  double v[10];
+  if (int rc = scal(c, c->partial, v, npt)) return rc;
+  for (int m = 0; m < npt; m++) mdata[m] += v[m];  // the reference accumulates into mdata
+  return ASKJA_OK;
+}
+
+int askja_Tab_all(askja_ctx* c, int npt, double* out) {
+  if (int rc = check_ctx(c)) return rc;
+  if (!out) return set_err(c, ASKJA_ERR_ARG, "null output");
+  DevGuard g(c->p.device);
+  // the staging buffer (V*DIM*NC*NC double2) holds V*(DIM+2) doubles
+  if (int rc = tab_range(c, 0, c->V, npt, (double*)c->staging)) return rc;
+  CK(cudaMemcpyAsync(out, c->staging, sizeof(double) * npt * (size_t)c->V, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return ASKJA_OK;
+}
+
 int askja_leapfrog(askja_ctx* c, int nsteps, double eps) {
   if (int rc = check_ctx(c)) return rc;
   if (nsteps < 1) return set_err(c, ASKJA_ERR_ARG, "nsteps must be >= 1");

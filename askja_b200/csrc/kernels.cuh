@@ -9,6 +9,7 @@
 #include "rows.cuh"
 #include "small.cuh"
 #include "pair.cuh"
+#include "tab.cuh"
 #include "eig.cuh"
 #include "tc.cuh"
 
@@ -415,10 +416,39 @@ cudaError_t to_conf(const LaunchCtx& c, const void* f, void* conf) {
   return cudaGetLastError();
 }
 
+// FourierTrafo (sun.cpp:365-411): plaquette energy of sites 0..n-1 (one CTA
+// per site), then |inverse DFT| of that sequence into coef[0..n-1].
+template <typename T>
+cudaError_t fourier(const LaunchCtx& c, const void* U, int n, double* partial, double* coef) {
+  using S2 = typename Storage<T>::type;
+  auto k = misc::k_plaq_big<S2>;
+  const size_t smem = 2 * (size_t)c.lat.N * (c.lat.N + 1) * sizeof(cpx<double>);
+  cudaError_t e;
+  if ((e = set_smem(k, smem)) != cudaSuccess) return e;
+  k<<<n, misc::RED_THREADS, smem, c.stream>>>(c.lat, (const S2*)U, partial);
+  tab::k_dft_abs<<<blocks_for(n, 128), 128, 0, c.stream>>>(partial, n, coef);
+  return cudaGetLastError();
+}
+
+// Tab (sun.cpp:580-670) for sites site0 .. site0+nsites-1: out[k*npt + m]
+template <typename T>
+cudaError_t tab_sites(const LaunchCtx& c, const void* U, const void* Pa, const void* Pb, int site0, int nsites,
+                      int npt, double* out) {
+  using S2 = typename Storage<T>::type;
+  if (c.lat.D > tab::TAB_MAX_D || c.lat.N > 64 || npt < 2 || npt > c.lat.D + 2) return cudaErrorInvalidValue;
+  auto k = tab::k_tab<S2>;
+  const size_t smem = tab::tab_smem(c.lat.N);
+  cudaError_t e;
+  if ((e = set_smem(k, smem)) != cudaSuccess) return e;
+  const int threads = 32 * ((c.lat.N + 31) / 32);
+  k<<<nsites, threads, smem, c.stream>>>(c.lat, (const S2*)U, (const S2*)Pa, (const S2*)Pb, site0, npt, out);
+  return cudaGetLastError();
+}
+
 template <typename T>
 constexpr KernelSet make_set() {
   return KernelSet{&force<T>,   &drift<T>,   &reunit<T>,  &plaq<T>,           &linksums<T>,  &gauss<T>, &lines<T>,
-                   &slice_trace<T>, &line_eigs<T>, &refresh<T>, &identity<T>, &gauss_matrices<T>, &from_conf<T>, &to_conf<T>, &pair_swap<T>};
+                   &slice_trace<T>, &line_eigs<T>, &refresh<T>, &identity<T>, &gauss_matrices<T>, &from_conf<T>, &to_conf<T>, &pair_swap<T>, &fourier<T>, &tab_sites<T>};
 }
 
 }  // namespace detail

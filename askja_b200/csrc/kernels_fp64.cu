@@ -14,7 +14,8 @@ size_t partial_doubles(const Lat& L) {
       2 * (size_t)L.N * L.N * ((nl + detail::GAUSS_LINKS_PER_BLOCK - 1) / detail::GAUSS_LINKS_PER_BLOCK);
   // one partial per site / per link for the large-NC reductions
   const size_t big = L.N >= misc::BIG_NC ? std::max(2 * (size_t)L.V, 3 * (size_t)nl) : 0;
-  return std::max(std::max(plaq, big), std::max(links, gauss)) + 64;
+  const size_t fourier = 2 * (size_t)L.n[0];  // FourierTrafo: one plaquette partial per site 0..N0-1
+  return std::max(std::max(std::max(plaq, big), std::max(links, gauss)), fourier) + 64;
 }
 
 int rows_effective_groups(int N, bool fp64, int want) {

@@ -63,6 +63,11 @@ struct KernelSet {
   cudaError_t (*to_conf)(const LaunchCtx&, const void* f, void* conf);
   // canonical <-> site-pair layout of a field, in place (FP32 only)
   cudaError_t (*pair_swap)(const LaunchCtx&, void* f);
+  // FourierTrafo: coef[0..n-1] (partial: 2n doubles of scratch)
+  cudaError_t (*fourier)(const LaunchCtx&, const void* U, int n, double* partial, double* coef);
+  // Tab for nsites sites from site0 with momenta Pa + Pb: out[k*npt + m]
+  cudaError_t (*tab)(const LaunchCtx&, const void* U, const void* Pa, const void* Pb, int site0, int nsites, int npt,
+                     double* out);
 };
 
 // size (in doubles) of the partial buffer the reductions need

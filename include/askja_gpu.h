@@ -147,6 +147,20 @@ ASKJA_API int askja_PolyakovLoop(askja_ctx* ctx, double* out);                 /
 ASKJA_API int askja_WilsonLoopDir(askja_ctx* ctx, int dir, double* out);       /* measurements4d.cpp:311-355 */
 ASKJA_API int askja_PlaqExp(askja_ctx* ctx, double* temporal, double* spatial);/* measurements4d.cpp:885-927 */
 ASKJA_API int askja_scalarLoopcorr(askja_ctx* ctx, double* out /* N0 values */); /* measurements4d.cpp:357-408 */
+
+/* ---- diagnostics the reference defines but never calls ---------------- */
+/* FourierTrafo (sun.cpp:365-411): coefficients[j] = |x_j|, x the inverse DFT
+ * (1/N0 normalised, as gsl_fft_complex_inverse) of the plaquette energy
+ * sum_{a<b} (1 - ReTr P_ab / NC) of sites 0 .. N0-1 (site numbers, as the
+ * reference loops them).  N0 values; NC <= 64. */
+ASKJA_API int askja_FourierTrafo(askja_ctx* ctx, double* coefficients);
+/* Tab (sun.cpp:580-670): adds site i's energy-momentum tensor terms, built
+ * from the clover field strength of u and from pi + Pi, to mdata[0..Npt-1]
+ * (mdata accumulates, as in the reference).  2 <= Npt <= DIM+2, DIM <= 8,
+ * NC <= 64. */
+ASKJA_API int askja_Tab(askja_ctx* ctx, long i, double* mdata, int Npt);
+/* Tab for every site: out[s*Npt + m] = site s's contribution to mdata[m]. */
+ASKJA_API int askja_Tab_all(askja_ctx* ctx, int Npt, double* out /* V*Npt */);
 /* getevs (measurements4d.cpp:185-309): eigenphases of the N0 Wilson lines
  * along direction 1 through (x0,0,..) and of the N1 Polyakov lines along
  * direction 0 through (0,x1,0,..); per line the NC phases arg(lambda) are

@@ -324,6 +324,16 @@ class Reference:
         self.sun.ref_Adjoint(_c(a.view(np.float64)), _c(out.view(np.float64)))
         return out
 
+    def Tab(self, i, npt, mdata=None):
+        m = np.zeros(npt) if mdata is None else np.ascontiguousarray(mdata, dtype=np.float64)
+        self.sun.ref_Tab(ctypes.c_long(int(i)), _c(m), ctypes.c_int(int(npt)))
+        return m
+
+    def FourierTrafo(self):
+        out = np.zeros(self.dims[0])
+        self.sun.ref_FourierTrafo(_c(out))
+        return out
+
     def getplus(self, ind, d):
         return self.sun.ref_getplus(int(ind), int(d))
 

@@ -19,6 +19,7 @@
 //   generators           sun.cpp:142-189
 //   mexpi / Adjoint      sunmat.h:200-248, 355-371
 //   getplus / getminus   structs.h:169-218
+//   Tab, FourierTrafo    sun.cpp:580-670, 365-411 (never called by the reference)
 // GSL and Eigen are replaced by the project-written shim under oracle/shim.
 #include <math.h>
 #include <omp.h>
@@ -152,3 +153,6 @@ EXPORT void ref_Adjoint(const double* a, double* out) {
   r = Adjoint(m);
   memcpy(out, r.M->data, (size_t)NC * NC * 2 * sizeof(double));
 }
+
+EXPORT void ref_Tab(long i, double* mdata, int npt) { Tab(i, mdata, npt); }
+EXPORT void ref_FourierTrafo(double* coefficients) { FourierTrafo(coefficients); }
