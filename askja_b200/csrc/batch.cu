@@ -179,6 +179,16 @@ template <typename T>
 int enqueue_trajectory(askja_batch* b, int nsteps) {
   using S2 = typename askja::Storage<T>::type;
   using namespace askja::batch;
+  for (int c = 0; c < b->nchains; c++) {  // gated full reunitarisation (d.reunit == 2)
+    const auto& d = b->desc[c];
+    if (d.reunit != 2) continue;
+    askja::LaunchCtx lc = chain_lc(b, c);
+    lc.gate = &d.st->traj;
+    lc.gate_every = askja::FULL_REUNIT_EVERY;
+    if (cudaError_t e = kset(b).reunit(lc, d.U[b->cur])) return berr(b, ASKJA_ERR_CUDA, "reunit: %s", cudaGetErrorString(e));
+    BCK(cudaMemcpyAsync(d.Uconf, d.U[b->cur], askja::field_elems(d.lat) * sizeof(askja::cpx<T>), cudaMemcpyDeviceToDevice,
+                        b->stream));
+  }
   kb_refresh<S2><<<b->n_refresh, 128, 0, b->stream>>>(b->d_desc, b->d_refresh_start, b->nchains);
   BCK(cudaGetLastError());
   if (int rc = energies<T>(b, 0)) return rc;
@@ -310,7 +320,10 @@ int askja_batch_create(const askja_chain_params* chains, int nchains, int precis
     d.beta = p.beta;
     d.scale = std::sqrt(2.0 * p.nc / p.beta);
     d.order = askja::taylor_order(p.level);
-    d.reunit = precision == ASKJA_FP32;
+    // FP32: reunitarise after each update; on the row kernels (NC > 4) by a
+    // Newton-Schulz step, with a full pass every FULL_REUNIT_EVERY
+    // trajectories, as a single chain does
+    d.reunit = precision == ASKJA_FP32 ? (p.nc > 4 ? 2 : 1) : 0;
     d.seed = p.seed;
     if (int rc = dalloc(b, &d.st, sizeof(TrajState))) return fail(rc);
     if (cudaMemset(d.st, 0, sizeof(TrajState)) != cudaSuccess) return fail(berr(b, ASKJA_ERR_CUDA, "memset"));

@@ -148,8 +148,10 @@ int launch_ok(askja_ctx* c, cudaError_t e, const char* what) {
     if (rc_) return rc_;                          \
   } while (0)
 
-// tensor-core path: trajectories between two Gram-Schmidt passes over U
-constexpr int TC_REUNIT_EVERY = 10;
+// whether the fused kick+drift runs on the row-per-thread kernels
+bool uses_rows(const askja_ctx* c) {
+  return c->lc.force_rows == 1 || (c->lc.force_rows == 0 && c->N > 4);
+}
 
 bool paired(const askja_ctx* c) { return c->lc.force_rows == 3; }
 
@@ -178,14 +180,16 @@ int fused_steps(askja_ctx* c, int n, double first_kick, double dt) {
 int enqueue_trajectory(askja_ctx* c, int nsteps) {
   const double dt = c->p.dt;
   const double scale = std::sqrt(2.0 * c->N / c->p.beta);
-  if (c->lc.force_rows == 2 && c->lc.reunit) {
+  if (c->lc.reunit && (c->lc.force_rows == 2 || (c->lc.rows_ns && uses_rows(c)))) {
     // the tensor-core link update keeps U' exactly as unitary as U (it
     // projects exp(i eps P), not U'); the rounding defect U accumulates (an
     // unbiased random walk, ~6e-8 sqrt(MD steps)) is removed here, before
-    // every TC_REUNIT_EVERY-th trajectory, and the saved copy follows
+    // every askja::FULL_REUNIT_EVERY-th trajectory, and the saved copy follows.  The
+    // FP32 row kernels project each update by a Newton-Schulz step, which
+    // leaves the determinant phase free; this pass pins it back to 1.
     askja::LaunchCtx lc = c->lc;
     lc.gate = &c->st->traj;
-    lc.gate_every = TC_REUNIT_EVERY;
+    lc.gate_every = askja::FULL_REUNIT_EVERY;
     KL(c->ks->reunit(lc, cur_u(c)), "reunitarise");
     KL(cudaMemcpyAsync(c->Uconf, cur_u(c), c->field_bytes, cudaMemcpyDeviceToDevice, c->stream), "save links");
   }
@@ -394,6 +398,7 @@ int askja_create(const askja_params* p, askja_ctx** out) {
   c->lc.stream = c->stream;
   c->lc.order = askja::taylor_order(p->level);
   c->lc.reunit = p->reunitarise < 0 ? (p->precision == ASKJA_FP32) : (p->reunitarise != 0);
+  c->lc.rows_ns = p->precision == ASKJA_FP32;
   CKC(cudaMalloc(&c->tc_status, sizeof(unsigned)));
   CKC(cudaMemset(c->tc_status, 0, sizeof(unsigned)));
   c->lc.scratch = c->staging;

@@ -64,8 +64,10 @@ cudaError_t rows_force(const LaunchCtx& c, int mode, const void* U, const void* 
   } else {
     auto k = rows::k_force<NMAX, T, S2, 1>;
     if ((e = set_smem(k, smem)) != cudaSuccess) return e;
+    // reunit 2: Newton-Schulz projection (FP32 single chains, see LaunchCtx::rows_ns)
+    const int ru = (sizeof(T) == 4 && c.reunit && c.rows_ns) ? 2 : c.reunit;
     k<<<grid, G * c.lat.N, smem, c.stream>>>(c.lat, (const S2*)U, (const S2*)Pin, (S2*)Pout, (S2*)Uout, (T)ek, (T)ed,
-                                             c.order, c.reunit);
+                                             c.order, ru);
   }
   return cudaGetLastError();
 }

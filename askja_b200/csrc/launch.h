@@ -15,6 +15,8 @@ struct LaunchCtx {
   cudaStream_t stream;
   int order;        // effective Taylor order
   int reunit;       // reunitarise after each link update
+  int rows_ns;      // row kernels, FP32: project by one Newton-Schulz step per update (the engine
+                    // re-orthonormalises with the determinant phase every few trajectories)
   int force_rows;   // kernel mapping: 0 thread-per-link (NC <= 4), 1 row-per-thread,
                     // 2 tensor cores (FP32, NC = 32 or 64, DIM >= 2), 3 site pairs in
                     // packed FP32 (NC = 3, even n[DIM-1]; the fused kick+drift then
@@ -27,6 +29,11 @@ struct LaunchCtx {
   const unsigned long long* gate;
   int gate_every;
 };
+
+// Trajectories between two full reunitarisation passes (Gram-Schmidt with the
+// determinant phase) over U, where the per-update projection leaves drift: the
+// tensor-core path and the FP32 row kernels (Newton-Schulz per update).
+constexpr int FULL_REUNIT_EVERY = 10;
 
 // whether the tensor-core mapping exists for this shape and precision
 inline bool tc_supported(int N, int D, bool fp64) { return !fp64 && (N == 32 || N == 64) && D >= 2; }

@@ -233,6 +233,53 @@ __device__ void reunitarise_tile(cpx<T>* S, cpx<T>* S2t, int N, int r, bool act,
   __syncthreads();
 }
 
+// One Newton-Schulz step towards the nearest unitary matrix,
+//   U <- U (3 - U^dag U) / 2,
+// the per-update projection of the FP32 single-chain path: after the link
+// update U is unitary to FP32 rounding and the step squares the defect, so it
+// returns to the rounding level; two tile products and three barriers instead
+// of reunitarise_tile's 4N.  It does not pin det U to 1: the engine runs the
+// full reunitarisation (with the determinant phase) over all links every few
+// trajectories.  tm: row r of U; the result rows go to T0 with stride N (the
+// copy-out layout).  All threads of the block call this (it has barriers).
+template <int NMAX, typename T>
+__device__ void newton_schulz_tile(const cpx<T> (&tm)[NMAX], cpx<T>* T0, cpx<T>* T1, int N, int NP, int r,
+                                   bool act) {
+  __syncthreads();
+  if (act) {
+#pragma unroll
+    for (int c = 0; c < NMAX; c++)
+      if (c < N) T0[r * NP + c] = tm[c];
+  }
+  __syncthreads();
+  if (act) {
+    cpx<T> a[NMAX], m[NMAX];
+#pragma unroll
+    for (int k = 0; k < NMAX; k++) {
+      m[k] = czero<T>();
+      if (k < N) {
+        const cpx<T> z = T0[k * NP + r];
+        a[k] = mkc<T>(z.re, -z.im);  // row r of U^dag
+      }
+    }
+    row_times_tile_acc<NMAX, T>(m, a, T0, NP, N);  // m[c] = (U^dag U)_rc
+#pragma unroll
+    for (int c = 0; c < NMAX; c++)
+      if (c < N) T1[r * NP + c] = mkc<T>((c == r ? T(1.5) : T(0)) - T(0.5) * m[c].re, T(-0.5) * m[c].im);
+  }
+  __syncthreads();
+  if (act) {
+    cpx<T> un[NMAX];
+#pragma unroll
+    for (int c = 0; c < NMAX; c++) un[c] = czero<T>();
+    row_times_tile_acc<NMAX, T>(un, tm, T1, NP, N);
+#pragma unroll
+    for (int c = 0; c < NMAX; c++)
+      if (c < N) T0[r * N + c] = un[c];
+  }
+  __syncthreads();
+}
+
 // MODE 0: out-of-place kick  Pout = Pin - eps_k F(U)
 // MODE 1: fused kick + drift P -= eps_k F(U); Uout = exp(i eps_d P) U
 //
@@ -402,16 +449,20 @@ __device__ __forceinline__ void force_rows(const Lat& L, const S2* __restrict__ 
         for (int c = 0; c < NMAX; c++) tm[c] = mkc<T>(fma(s[c].re, inv, u[c].re), fma(s[c].im, inv, u[c].im));
       }
     }
-    __syncthreads();
-    if (act) {
+    if (reunit == 2) {  // Newton-Schulz projection (ends with a barrier)
+      newton_schulz_tile<NMAX, T>(tm, T0, T1, N, NP, r, act);
+    } else {
+      __syncthreads();
+      if (act) {
 #pragma unroll
-      for (int c = 0; c < NMAX; c++)
-        if (c < N) T0[r * N + c] = tm[c];
+        for (int c = 0; c < NMAX; c++)
+          if (c < N) T0[r * N + c] = tm[c];
+      }
+      __syncthreads();
+      if (reunit) reunitarise_tile<T>(T0, T0 + N * N, N, r, act, &piv_s[act ? g : 0], &det_s[act ? g : 0]);
+      // copy out (reunitarise_tile ends with a barrier)
+      if (!reunit) __syncthreads();
     }
-    __syncthreads();
-    if (reunit) reunitarise_tile<T>(T0, T0 + N * N, N, r, act, &piv_s[act ? g : 0], &det_s[act ? g : 0]);
-    // copy out (reunitarise_tile ends with a barrier)
-    if (!reunit) __syncthreads();
     if (cact) {
 #pragma unroll
       for (int c = 0; c < NMAX; c++)
