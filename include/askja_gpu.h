@@ -63,7 +63,11 @@ typedef struct {
   double dt;           /* DT (used by askja_trajectory) */
   int level;           /* LEVEL: Taylor order of exp(i dt P); outside 0..8 acts as 8 (sunmat.h:215-246) */
   int precision;       /* ASKJA_FP64 or ASKJA_FP32 */
-  int reunitarise;     /* -1 default (on for FP32, off for FP64), 0 off, 1 on */
+  int reunitarise;     /* -1 default (on for FP32, off for FP64), 0 off, 1 on.  On: every
+                          link update is projected back onto SU(NC); the FP32 row kernels
+                          (NC > 4) and tensor cores project onto U(NC) per update and
+                          askja_trajectory / askja_run_trajectories run the full SU(NC)
+                          projection before every 10th trajectory */
   int device;          /* CUDA device ordinal */
   int kernel_path;     /* 0 automatic; 1 row-per-thread kernels for every NC (testing);
                           2 tensor cores (FP32 with NC = 32 or 64 and DIM >= 2 only);
