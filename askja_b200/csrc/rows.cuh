@@ -280,6 +280,85 @@ __device__ void newton_schulz_tile(const cpx<T> (&tm)[NMAX], cpx<T>* T0, cpx<T>*
   __syncthreads();
 }
 
+// Tm = sum_{k<=order} X^k/k! U by Paterson-Stockmeyer with block size 3:
+// with X^3 staged once, E = (..(B_q X^3 + B_(q-1)) X^3 + ..) X^3 + B_0
+// (formed without its identity term, Tm = U + (E - 1) U),
+// B_j = sum_{i<3} X^i / (3j+i)!, needs X^2, X^3, q = order/3 block products
+// and E U -- 5 tile products for order 8 instead of Horner's 8, and three
+// barriers instead of two per product (the block steps multiply by the same
+// staged X^3).  Exact in real arithmetic; p = row r of X, u = row r of U.
+// All threads of the block call this (it has barriers).
+template <int NMAX, typename T>
+__device__ void drift_ps(cpx<T> (&tm)[NMAX], const cpx<T> (&p)[NMAX], const cpx<T> (&u)[NMAX], cpx<T>* T0,
+                         cpx<T>* T1, cpx<T>* T2, int N, int NP, int r, bool act, int order) {
+  __syncthreads();
+  if (act) {
+#pragma unroll
+    for (int c = 0; c < NMAX; c++)
+      if (c < N) {
+        T0[r * NP + c] = p[c];
+        T2[r * NP + c] = u[c];
+      }
+  }
+  __syncthreads();
+  cpx<T> x2[NMAX];
+#pragma unroll
+  for (int c = 0; c < NMAX; c++) x2[c] = czero<T>();
+  if (act) {
+    row_times_tile_acc<NMAX, T>(x2, p, T0, NP, N);
+    cpx<T> x3[NMAX];
+#pragma unroll
+    for (int c = 0; c < NMAX; c++) x3[c] = czero<T>();
+    row_times_tile_acc<NMAX, T>(x3, x2, T0, NP, N);
+#pragma unroll
+    for (int c = 0; c < NMAX; c++)
+      if (c < N) T1[r * NP + c] = x3[c];
+  }
+  __syncthreads();
+  if (act) {
+    // 1/k! for k <= order, zero beyond
+    auto invfact = [order](int k) {
+      if (k > order) return T(0);
+      T f = T(1);
+      for (int i = 2; i <= k; i++) f = f / T(i);
+      return f;
+    };
+    const int q = order / 3;
+    cpx<T> acc[NMAX];
+    for (int j = q; j >= 0; j--) {
+      // the identity of B_0 is left out: Em = E - 1, and U' = U + Em U keeps
+      // the small update apart from U's own bits
+      const T a0 = j ? invfact(3 * j) : T(0), a1 = invfact(3 * j + 1), a2 = invfact(3 * j + 2);
+      cpx<T> nb[NMAX];  // B_j (+ acc X^3)
+#pragma unroll
+      for (int c = 0; c < NMAX; c++)
+        nb[c] = mkc<T>(fma(a2, x2[c].re, fma(a1, p[c].re, c == r ? a0 : T(0))), fma(a2, x2[c].im, a1 * p[c].im));
+      if (j < q) row_times_tile_acc<NMAX, T>(nb, acc, T1, NP, N);
+#pragma unroll
+      for (int c = 0; c < NMAX; c++) acc[c] = nb[c];
+    }
+#pragma unroll
+    for (int c = 0; c < NMAX; c++) tm[c] = u[c];
+    row_times_tile_acc<NMAX, T>(tm, acc, T2, NP, N);
+  }
+}
+
+// Rows of the updated link -> T0 (stride N), then the full reunitarisation
+// when reunit (ends with a barrier either way).
+template <int NMAX, typename T>
+__device__ __forceinline__ void finish_update(const cpx<T> (&tm)[NMAX], cpx<T>* T0, int N, int r, bool act,
+                                              int reunit, int* piv, cpx<T>* det) {
+  __syncthreads();
+  if (act) {
+#pragma unroll
+    for (int c = 0; c < NMAX; c++)
+      if (c < N) T0[r * N + c] = tm[c];
+  }
+  __syncthreads();
+  if (reunit) reunitarise_tile<T>(T0, T0 + N * N, N, r, act, piv, det);
+  if (!reunit) __syncthreads();
+}
+
 // MODE 0: out-of-place kick  Pout = Pin - eps_k F(U)
 // MODE 1: fused kick + drift P -= eps_k F(U); Uout = exp(i eps_d P) U
 //
@@ -431,7 +510,13 @@ __device__ __forceinline__ void force_rows(const Lat& L, const S2* __restrict__ 
       tm[c] = u[c];
       p[c] = mkc<T>(-eps_d * p[c].im, eps_d * p[c].re);
     }
-    for (int n = order; n >= 1; n--) {
+    // FP32, NC <= 8, order >= 5: the same series by Paterson-Stockmeyer (the
+    // Horner loop below is then skipped; for larger NC its extra row arrays
+    // cost more occupancy than it saves); FP64 keeps the reference's Horner order
+    const bool ps = sizeof(T) == 4 && NMAX == 8 && order >= 5;
+    if constexpr (sizeof(T) == 4 && NMAX == 8)
+      if (ps) drift_ps<NMAX, T>(tm, p, u, T0, T1, T2, N, NP, r, act, order);
+    for (int n = ps ? 0 : order; n >= 1; n--) {
       __syncthreads();
       if (act) {
 #pragma unroll
@@ -449,19 +534,13 @@ __device__ __forceinline__ void force_rows(const Lat& L, const S2* __restrict__ 
         for (int c = 0; c < NMAX; c++) tm[c] = mkc<T>(fma(s[c].re, inv, u[c].re), fma(s[c].im, inv, u[c].im));
       }
     }
-    if (reunit == 2) {  // Newton-Schulz projection (ends with a barrier)
-      newton_schulz_tile<NMAX, T>(tm, T0, T1, N, NP, r, act);
+    if constexpr (sizeof(T) == 4) {
+      if (reunit == 2)  // Newton-Schulz projection (ends with a barrier)
+        newton_schulz_tile<NMAX, T>(tm, T0, T1, N, NP, r, act);
+      else
+        finish_update<NMAX, T>(tm, T0, N, r, act, reunit, &piv_s[act ? g : 0], &det_s[act ? g : 0]);
     } else {
-      __syncthreads();
-      if (act) {
-#pragma unroll
-        for (int c = 0; c < NMAX; c++)
-          if (c < N) T0[r * N + c] = tm[c];
-      }
-      __syncthreads();
-      if (reunit) reunitarise_tile<T>(T0, T0 + N * N, N, r, act, &piv_s[act ? g : 0], &det_s[act ? g : 0]);
-      // copy out (reunitarise_tile ends with a barrier)
-      if (!reunit) __syncthreads();
+      finish_update<NMAX, T>(tm, T0, N, r, act, reunit, &piv_s[act ? g : 0], &det_s[act ? g : 0]);
     }
     if (cact) {
 #pragma unroll
@@ -483,6 +562,22 @@ __global__ void k_force(Lat L, const S2* __restrict__ U, const S2* Pin, S2* Pout
   const int site0 = (blockIdx.x / L.D) * GS;
   force_rows<NMAX, T, S2, MODE>(L, U, Pin, Pout, Uout, eps_k, eps_d, order, reunit, mu, site0, smem_raw, piv_s,
                                 det_s);
+}
+
+// The same for FP32 with NMAX = 8 (the Paterson-Stockmeyer drift): at most 128
+// registers, so that four 128-thread CTAs stay resident per SM.
+template <typename S2, int MODE>
+__global__ void __launch_bounds__(256, 2) k_force8(Lat L, const S2* __restrict__ U, const S2* Pin, S2* Pout,
+                                                   S2* __restrict__ Uout, float eps_k, float eps_d, int order,
+                                                   int reunit) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ int piv_s[64];
+  __shared__ cpx<float> det_s[64];
+  const int GS = blockDim.x / L.N;
+  const int mu = blockIdx.x % L.D;
+  const int site0 = (blockIdx.x / L.D) * GS;
+  force_rows<8, float, S2, MODE>(L, U, Pin, Pout, Uout, eps_k, eps_d, order, reunit, mu, site0, smem_raw, piv_s,
+                                 det_s);
 }
 
 // In-place drift U <- exp(i eps P) U, optional reunitarisation.
