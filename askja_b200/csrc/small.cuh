@@ -343,7 +343,8 @@ __device__ __forceinline__ void expi_times_ch(Mat<N, T>& Tm, const Mat<N, T>& P,
 //   a_k = -d g_(k-1),  b_k = a_(k-1) + c1 g_(k-1),  g_k = b_(k-1) + tau g_(k-1),
 // and  E = A 1 + B P + C P^2  with  A = sum i^k a_k/k!, B = eps sum i^k b_k/k!,
 // C = eps^2 sum i^k g_k/k!.  P^2 is Hermitian: its upper triangle and real
-// diagonal are formed (no X, no full X^2 product).
+// diagonal are formed (no X, no full X^2 product).  E - 1 is formed and the
+// result is U + (E - 1) U.
 template <typename T>
 __device__ __forceinline__ void expi_times_herm3(Mat<3, T>& Tm, const Mat<3, T>& P, const Mat<3, T>& Ux, T eps,
                                                  int order) {
@@ -374,7 +375,9 @@ __device__ __forceinline__ void expi_times_herm3(Mat<3, T>& Tm, const Mat<3, T>&
   const T c1 = T(0.5) * fma(eps * eps, trq, -tau * tau);
   const T d = -(eps * eps * eps) * det;
   T a = T(1), b = T(0), g = T(0);
-  cpx<T> A = mkc<T>(T(1), T(0)), B = czero<T>(), C = czero<T>();
+  // A without its k = 0 term: E - 1 is formed, and Tm = U + (E - 1) U keeps the
+  // small update apart from U's own bits
+  cpx<T> A = czero<T>(), B = czero<T>(), C = czero<T>();
   T f = T(1);
 #pragma unroll
   for (int k = 1; k <= 8; k++) {  // order <= 8; unrolled so that 1/k! and i^k are constants
@@ -421,7 +424,8 @@ __device__ __forceinline__ void expi_times_herm3(Mat<3, T>& Tm, const Mat<3, T>&
     cmac_nc(l, C, Qu[u]);
     E.a[j][i] = l;
   }
-  mul_nn(Tm, E, Ux);
+  Tm = Ux;
+  mac_nn(Tm, E, Ux);
 }
 
 // Link update of the FP32 path: the Cayley-Hamilton form (for N = 3 in P,
