@@ -46,6 +46,7 @@ EXPORTS = [
     "askja_batch_hot_start", "askja_batch_set_links", "askja_batch_get_links", "askja_batch_run",
     "askja_batch_plaquette", "askja_autotune", "askja_set_tuning", "askja_set_links_async", "askja_trajectory_async",
     "askja_FourierTrafo", "askja_Tab", "askja_Tab_all",
+    "askja_force_step", "askja_link_step", "askja_action", "askja_kinetic", "askja_refresh_momenta", "askja_measure",
 ]
 
 
@@ -125,6 +126,11 @@ def library() -> ctypes.CDLL:
     L.askja_PlaqExp.argtypes = [vp, dp, dp]
     L.askja_eigenphases.argtypes = [vp, dp, dp]
     L.askja_FourierTrafo.argtypes = [vp, dp]
+    for name in ("askja_force_step", "askja_link_step"):
+        getattr(L, name).argtypes = [vp, ctypes.c_double]
+    for name in ("askja_action", "askja_kinetic", "askja_measure"):
+        getattr(L, name).argtypes = [vp, dp]
+    L.askja_refresh_momenta.argtypes = [vp, ctypes.c_uint64, ctypes.c_uint64]
     L.askja_Tab.argtypes = [vp, ctypes.c_long, dp, ip]
     L.askja_Tab_all.argtypes = [vp, ip, dp]
     L.askja_trajectory.argtypes = [vp, ip, ctypes.POINTER(TrajResult)]
@@ -321,6 +327,12 @@ class Engine:
     def scalarLoopcorr(self):
         out = np.zeros(self.dims[0])
         self._ck(self.lib.askja_scalarLoopcorr(self._ctx, _dptr(out)))
+        return out
+
+    def measure(self):
+        """askja_measure: [plaq_t, plaq_s, polyakov, wilson(1..DIM-1), gauss, uviol]."""
+        out = np.zeros(self.dim + 4)
+        self._ck(self.lib.askja_measure(self._ctx, _dptr(out)))
         return out
 
     def FourierTrafo(self):

@@ -728,6 +728,27 @@ int askja_scalarLoopcorr(askja_ctx* c, double* out) {
   return scal(c, c->lines, out, c->lat.n[0]);
 }
 
+// Short names for the seam functions (same calls, same semantics).
+int askja_force_step(askja_ctx* c, double eps) { return askja_updateE(c, eps); }
+int askja_link_step(askja_ctx* c, double eps) { return askja_updateUandcopyDown(c, eps); }
+int askja_action(askja_ctx* c, double* s_over_beta) { return askja_EnergyMag(c, s_over_beta); }
+int askja_kinetic(askja_ctx* c, double* trp2) { return askja_simpleenergyEl(c, 0, trp2); }
+int askja_refresh_momenta(askja_ctx* c, uint64_t seed, uint64_t counter) {
+  return askja_initializeE(c, seed, counter);
+}
+
+int askja_measure(askja_ctx* c, double* out) {
+  if (int rc = check_ctx(c)) return rc;
+  if (!out) return set_err(c, ASKJA_ERR_ARG, "null output");
+  if (c->D < 2) return set_err(c, ASKJA_ERR_ARG, "askja_measure needs DIM >= 2");
+  if (int rc = askja_PlaqExp(c, out, out + 1)) return rc;
+  if (int rc = askja_PolyakovLoop(c, out + 2)) return rc;
+  for (int d = 1; d < c->D; d++)
+    if (int rc = askja_WilsonLoopDir(c, d, out + 2 + d)) return rc;
+  if (int rc = askja_GaussLaw(c, out + c->D + 2)) return rc;
+  return askja_UViol(c, out + c->D + 3);
+}
+
 int askja_FourierTrafo(askja_ctx* c, double* coefficients) {
   if (int rc = check_ctx(c)) return rc;
   if (!coefficients) return set_err(c, ASKJA_ERR_ARG, "null output");

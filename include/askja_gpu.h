@@ -152,6 +152,18 @@ ASKJA_API int askja_WilsonLoopDir(askja_ctx* ctx, int dir, double* out);       /
 ASKJA_API int askja_PlaqExp(askja_ctx* ctx, double* temporal, double* spatial);/* measurements4d.cpp:885-927 */
 ASKJA_API int askja_scalarLoopcorr(askja_ctx* ctx, double* out /* N0 values */); /* measurements4d.cpp:357-408 */
 
+/* ---- short names for the seam (the same calls as above) --------------- */
+ASKJA_API int askja_force_step(askja_ctx* ctx, double eps);          /* = askja_updateE (sun.cpp:672-723) */
+ASKJA_API int askja_link_step(askja_ctx* ctx, double eps);           /* = askja_updateUandcopyDown (sun.cpp:774-790) */
+ASKJA_API int askja_action(askja_ctx* ctx, double* s_over_beta);     /* = askja_EnergyMag (sun.cpp:507-537) */
+ASKJA_API int askja_kinetic(askja_ctx* ctx, double* trp2);           /* = askja_simpleenergyEl(ctx, 0, .) (sun.cpp:540-548) */
+ASKJA_API int askja_refresh_momenta(askja_ctx* ctx, uint64_t seed, uint64_t counter); /* = askja_initializeE */
+/* The measurements of one configuration (DIM >= 2), DIM+4 values:
+ * out[0], out[1] PlaqExp temporal / spatial; out[2] PolyakovLoop;
+ * out[2+d] WilsonLoop(dir d), d = 1..DIM-1 (measurements4d.cpp:311-466, 885-927);
+ * out[DIM+2] GaussLaw; out[DIM+3] UViol (sun.cpp:415-471). */
+ASKJA_API int askja_measure(askja_ctx* ctx, double* out);
+
 /* ---- diagnostics the reference defines but never calls ---------------- */
 /* FourierTrafo (sun.cpp:365-411): coefficients[j] = |x_j|, x the inverse DFT
  * (1/N0 normalised, as gsl_fft_complex_inverse) of the plaquette energy
