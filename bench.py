@@ -335,8 +335,12 @@ def run_ours(args):
                     "fp32": {"flops_per_launch": fpl * links, "achieved": tf32, "peak": pk32, "unit": "TFLOP/s",
                              "frac": tf32 / pk32,
                              "peak_source": "measured FFMA on this device (askja_peak_flops)",
-                             "note": "matrix-product flops only (Cayley-Hamilton scalars, projection, "
-                                     "reunitarisation not counted)"}}
+                             "note": "matrix-product flops this kernel performs (Cayley-Hamilton scalars, "
+                                     "projection, reunitarisation not counted)",
+                             # the reference algorithm's count, 8 N^3 (4D + L - 2): L Horner products + E U
+                             "reference_algorithm_flops_per_launch": 8 * nc ** 3 * (4 * len(dims) + order - 2) * links,
+                             "frac_reference_algorithm": 8 * nc ** 3 * (4 * len(dims) + order - 2) * links
+                             / (f32["kernel_ms"] / 1e3) / 1e12 / pk32}}
     field_mb = links * nc * nc * 8 / 1e6
     line = {
         "metric": f"link-updates/s (1 B200): FP32-mixed HMC trajectories, SU({nc}) {'x'.join(map(str, dims))}",
