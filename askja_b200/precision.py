@@ -34,20 +34,22 @@ def _binned_error(x: np.ndarray, nbins: int = 10) -> float:
     return float(b.std(ddof=1) / np.sqrt(nbins))
 
 
-def thermalise(nc, dims, beta, dt, level, nsteps, ntraj, seed, device=0):
+def thermalise(nc, dims, beta, dt, level, nsteps, ntraj, seed, device=0, reunitarise=None, kernel_path=0):
     """Hot start, then `ntraj` FP32-mixed trajectories; returns FP64 U-conf links."""
-    with Engine(nc, dims, beta=beta, dt=dt, level=level, precision="fp32", device=device, seed=seed) as e:
+    with Engine(nc, dims, beta=beta, dt=dt, level=level, precision="fp32", device=device, seed=seed,
+                reunitarise=reunitarise, kernel_path=kernel_path) as e:
         e.hot_start(seed + 1)
         if ntraj:
             e.run_trajectories(ntraj, nsteps, use_graph=True, want_log=False)
         return e.get_links()
 
 
-def compare(nc, dims, beta, dt, level, nsteps, u0, ntraj_dh=3, seed=7, device=0):
+def compare(nc, dims, beta, dt, level, nsteps, u0, ntraj_dh=3, seed=7, device=0, reunitarise=None, kernel_path=0):
     out = {}
     kw = dict(beta=beta, dt=dt, level=level, device=device)
     with Engine(nc, dims, precision="fp64", seed=seed, **kw) as e64, \
-            Engine(nc, dims, precision="fp32", seed=seed, **kw) as e32:
+            Engine(nc, dims, precision="fp32", seed=seed, reunitarise=reunitarise, kernel_path=kernel_path,
+                   **kw) as e32:
         # one force evaluation on identical inputs
         e64.set_links(u0)
         e64.initializeE(seed, 12345)
@@ -79,6 +81,7 @@ def compare(nc, dims, beta, dt, level, nsteps, u0, ntraj_dh=3, seed=7, device=0)
                 out["links_max_dev_fp32_vs_fp64"] = float(np.abs(e32.get_links() - e64.get_links()).max())
         out["dH"] = rows
         out["max_abs_dH_diff"] = max(r["abs_diff"] for r in rows)
+        out["mean_signed_dH_diff"] = float(np.mean([r["dH32"] - r["dH64"] for r in rows]))
         # reversibility
         rev = {}
         for name, e in (("fp64", e64), ("fp32", e32)):
@@ -92,7 +95,7 @@ def compare(nc, dims, beta, dt, level, nsteps, u0, ntraj_dh=3, seed=7, device=0)
     return out
 
 
-def ensemble(nc, dims, beta, dt, level, nsteps, u0, ntraj, seed=11, device=0):
+def ensemble(nc, dims, beta, dt, level, nsteps, u0, ntraj, seed=11, device=0, reunitarise=None, kernel_path=0):
     res = {}
     vol = int(np.prod(dims))
     D = len(dims)
@@ -100,7 +103,8 @@ def ensemble(nc, dims, beta, dt, level, nsteps, u0, ntraj, seed=11, device=0):
     nt, ns = vol * (D - 1), vol * (D - 1) * (D - 2) // 2  # temporal (0,k) / spatial (j,k) planes
     obs = ("plaquette", "plaquette_t", "plaquette_s", "polyakov", "wilson")
     for prec in ("fp64", "fp32"):
-        with Engine(nc, dims, beta=beta, dt=dt, level=level, precision=prec, device=device, seed=seed) as e:
+        extra = dict(reunitarise=reunitarise, kernel_path=kernel_path) if prec == "fp32" else {}
+        with Engine(nc, dims, beta=beta, dt=dt, level=level, precision=prec, device=device, seed=seed, **extra) as e:
             e.set_links(u0)
             series = {k: [] for k in obs}
             acc = 0
@@ -140,13 +144,17 @@ def main():
     ap.add_argument("--dh-traj", type=int, default=5)
     ap.add_argument("--ensemble", type=int, default=0, help="trajectories per precision for <plaq>, <|P|>")
     ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--fp32-reunit", choices=["default", "on", "off"], default="default",
+                    help="FP32 engines: per-update reunitarisation (default: on)")
+    ap.add_argument("--fp32-path", type=int, default=0, help="FP32 engines: askja kernel_path")
     a = ap.parse_args()
+    kw = dict(reunitarise={"default": None, "on": True, "off": False}[a.fp32_reunit], kernel_path=a.fp32_path)
     t0 = time.perf_counter()
-    u0 = thermalise(a.nc, a.dims, a.beta, a.dt, a.level, a.nsteps, a.therm, a.seed)
+    u0 = thermalise(a.nc, a.dims, a.beta, a.dt, a.level, a.nsteps, a.therm, a.seed, **kw)
     rep = {"config": vars(a), "therm_seconds": time.perf_counter() - t0}
-    rep.update(compare(a.nc, a.dims, a.beta, a.dt, a.level, a.nsteps, u0, a.dh_traj))
+    rep.update(compare(a.nc, a.dims, a.beta, a.dt, a.level, a.nsteps, u0, a.dh_traj, **kw))
     if a.ensemble:
-        rep["ensemble"] = ensemble(a.nc, a.dims, a.beta, a.dt, a.level, a.nsteps, u0, a.ensemble)
+        rep["ensemble"] = ensemble(a.nc, a.dims, a.beta, a.dt, a.level, a.nsteps, u0, a.ensemble, **kw)
     print(json.dumps(rep))
 
 
