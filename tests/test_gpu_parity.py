@@ -104,7 +104,8 @@ def test_fp32_matches_golden(golden):
 
 
 CASES = [(2, [6, 4, 3, 5]), (3, [4, 4, 4, 4]), (3, [5, 1, 2, 3]), (4, [3, 4, 5]), (5, [3, 3, 2, 2]),
-         (6, [2, 3, 4]), (8, [3, 3, 2, 2]), (9, [2, 2, 3]), (12, [2, 2, 2]), (16, [2, 3])]
+         (6, [2, 3, 4]), (8, [3, 3, 2, 2]), (9, [2, 2, 3]), (12, [2, 2, 2]), (16, [2, 3]),
+         (3, [7]), (5, [4])]  # DIM 1: no plaquettes, zero force
 
 
 @pytest.mark.parametrize("nc,dims", CASES, ids=[f"su{n}_{'x'.join(map(str, d))}" for n, d in CASES])
