@@ -920,10 +920,7 @@ int askja_autotune(askja_ctx* c, int reps, askja_tuning* out) {
     cands.push_back({0, 0, 2});
   }
   if (askja::tc_supported(c->N, c->D, fp64)) cands.push_back({2, 0, 0});
-  if (askja::pair_supported(c->N, c->D, fp64, c->lat.n[c->D - 1])) {
-    cands.push_back({3, 0, 0});
-    cands.push_back({3, 0, 1});
-  }
+
   std::vector<int> seen;
   for (int want : {0, 2, 4, 8, 16, 32, 64}) {
     const int eff = askja::rows_effective_groups(c->N, fp64, want);
