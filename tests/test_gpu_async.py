@@ -39,7 +39,7 @@ def test_upload_matches_set_links(precision):
 
 
 @pytest.mark.parametrize("nc,dims,precision", [(3, [4, 4, 4, 4], "fp32"), (3, [4, 3, 4], "fp64"),
-                                               (8, [3, 4, 2], "fp32")])
+                                               (8, [3, 4, 2], "fp32"), (32, [2, 2, 2], "fp32")])
 def test_pipeline_matches_synchronous_calls(nc, dims, precision):
     """Five configurations through two host buffers: upload k+1 is enqueued
     while trajectory k runs; each trajectory's outcome and the final links
