@@ -119,6 +119,15 @@ cudaError_t launch_force(askja_batch* b, const askja_batch::Group& g, cudaStream
     int maxd = 1;
     for (int c : g.chains) maxd = std::max(maxd, b->desc[c].lat.D);
     const dim3 blk(32 * std::min(maxd, 4));
+    if constexpr (sizeof(T) == 4) {
+      if (g.N == 3) {
+        if (mode)
+          kb_force_small3f<1><<<grid, blk, 0, st>>>(b->d_desc, g.d_start, g.d_ids, (int)g.chains.size(), b->cur, ks);
+        else
+          kb_force_small3f<0><<<grid, blk, 0, st>>>(b->d_desc, g.d_start, g.d_ids, (int)g.chains.size(), b->cur, ks);
+        return cudaGetLastError();
+      }
+    }
 #define SMALL(NN)                                                                                            \
   if (g.N == NN) {                                                                                           \
     if (mode)                                                                                                \

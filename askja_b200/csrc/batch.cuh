@@ -7,6 +7,8 @@
 // of different sizes therefore share the GPU in proportion to their work.
 #pragma once
 
+#include <type_traits>
+
 #include "misc.cuh"
 #include "rows.cuh"
 #include "small.cuh"
@@ -64,23 +66,45 @@ __device__ __forceinline__ int load_chain(ChainDev& sd, const ChainDev* __restri
 
 // Force (+ link update) for the small-NC chains of one colour number: item =
 // 32-site tile, 32*min(D,4) threads (see small::k_force).
-template <int N, typename T, int MODE>
-__global__ void __launch_bounds__(128) kb_force_small(const ChainDev* __restrict__ descs,
-                                                      const int* __restrict__ item_start,
-                                                      const int* __restrict__ chain_ids, int nchains, int cur,
-                                                      double kick_scale) {
+// BYVAL: the geometry by value, so that the fields the force uses (V, B, D,
+// nbr) live in registers instead of being re-read from shared memory at every
+// address (costs registers; used where the register budget is fixed anyway)
+template <int N, typename T, int MODE, bool BYVAL>
+__device__ __forceinline__ void force_small_item(const ChainDev* __restrict__ descs,
+                                                 const int* __restrict__ item_start,
+                                                 const int* __restrict__ chain_ids, int nchains, int cur,
+                                                 double kick_scale) {
   using S2 = typename Storage<T>::type;
   __shared__ ChainDev sd;
   const int tile = load_chain(sd, descs, item_start, chain_ids, nchains);
-  const Lat& L = sd.lat;
+  using LatRef = typename std::conditional<BYVAL, const Lat, const Lat&>::type;
+  LatRef L = sd.lat;
   const int x = tile * 32 + (threadIdx.x & 31);
   if (x >= L.V) return;
   const S2* U = (const S2*)sd.U[cur];
   S2* P = (S2*)sd.P;
   S2* Uo = (S2*)sd.U[cur ^ 1];
+  const T ek = (T)(kick_scale * sd.dt), ed = (T)sd.dt;
+  const int order = sd.order, reunit = sd.reunit;
   for (int mu = threadIdx.x >> 5; mu < L.D; mu += (blockDim.x >> 5))
-    small::force_link<N, T, S2, MODE>(L, U, P, P, Uo, (T)(kick_scale * sd.dt), (T)sd.dt, sd.order, sd.reunit, mu,
-                                      x);
+    small::force_link<N, T, S2, MODE>(L, U, P, P, Uo, ek, ed, order, reunit, mu, x);
+}
+
+template <int N, typename T, int MODE>
+__global__ void __launch_bounds__(128) kb_force_small(const ChainDev* __restrict__ descs,
+                                                      const int* __restrict__ item_start,
+                                                      const int* __restrict__ chain_ids, int nchains, int cur,
+                                                      double kick_scale) {
+  force_small_item<N, T, MODE, false>(descs, item_start, chain_ids, nchains, cur, kick_scale);
+}
+
+// FP32 SU(3): seven resident CTAs per SM, as the single-chain kernel's tuned budget
+template <int MODE>
+__global__ void __launch_bounds__(128, 7) kb_force_small3f(const ChainDev* __restrict__ descs,
+                                                           const int* __restrict__ item_start,
+                                                           const int* __restrict__ chain_ids, int nchains, int cur,
+                                                           double kick_scale) {
+  force_small_item<3, float, MODE, true>(descs, item_start, chain_ids, nchains, cur, kick_scale);
 }
 
 // Same for the row-per-thread path: item = G consecutive sites of one

@@ -521,6 +521,13 @@ def batch_chains(n=64, seed=7):
     return chains
 
 
+def batch_su3_32_chains():
+    """Four SU(3) 32^4 chains, a beta scan (5.85 .. 6.15) at the headline
+    volume: DT 0.02, LEVEL 6 as the single-chain workload."""
+    return [dict(nc=3, dims=[32] * 4, beta=b, dt=0.02, level=6, seed=2000 + i)
+            for i, b in enumerate((5.85, 5.95, 6.05, 6.15))]
+
+
 def tune_dt(chains, nsteps, rounds=3, ntraj=6, dev=0):
     """Adjust each chain's DT towards ~80 % acceptance (FP32 batch, untimed)."""
     import askja_b200 as ab
@@ -540,15 +547,17 @@ def tune_dt(chains, nsteps, rounds=3, ntraj=6, dev=0):
 
 
 def run_batch(args):
-    """Config 'batch64': all chains in one batch (FP32-mixed) vs each chain
-    alone in FP64 through the single-chain engine."""
+    """Configs 'batch64' and 'batch_su3_32': all chains in one batch
+    (FP32-mixed) vs each chain alone in FP64 (and FP32) through the
+    single-chain engine."""
     import torch
 
     import askja_b200 as ab
     dev = 0
     torch.cuda.set_device(dev)
-    nsteps = 20
-    chains = tune_dt(batch_chains(), nsteps, dev=dev)
+    su3 = args.config == "batch_su3_32"
+    nsteps = 50 if su3 else 20
+    chains = batch_su3_32_chains() if su3 else tune_dt(batch_chains(), nsteps, dev=dev)
     work = sum(int(np.prod(c["dims"])) * len(c["dims"]) for c in chains) * nsteps
     with ab.Batch(chains, precision="fp32", device=dev) as b:
         b.hot_start(5)
@@ -581,15 +590,21 @@ def run_batch(args):
                 z.synchronize()
                 tot_ms += a.elapsed_time(z)
         alone[prec] = work * args.steps / (tot_ms / 1e3)
+    if su3:
+        metric = "link-updates/s (1 B200): 4 SU(3) 32^4 chains, FP32-mixed batched vs each chain alone in FP64"
+        workload = (f"batch_su3_32: 4 chains SU(3) DIM=4 32^4, BETA 5.85/5.95/6.05/6.15, DT=0.02, LEVEL=6, "
+                    f"{nsteps} MD steps/trajectory, 1 step = 1 trajectory of every chain")
+    else:
+        metric = "link-updates/s (1 B200): 64 uneven chains, FP32-mixed batched vs each chain alone in FP64"
+        workload = ("batch64: NC in {2,3,4,8}, DIM in {2,3,4}, 16^2..16^4 incl. 4x16^3, "
+                    f"BETA in [2,4]*NC^2/3, {nsteps} MD steps/trajectory, DT tuned per chain, "
+                    "1 step = 1 trajectory of every chain")
     return {
-        "metric": "link-updates/s (1 B200): 64 uneven chains, FP32-mixed batched vs each chain alone in FP64",
+        "metric": metric,
         "value": batched, "unit": "link-updates/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "fp32 (links) / fp64 (dH)", "data": "synthetic: Haar hot start, Philox momenta",
-        "config": {"workload": "batch64: NC in {2,3,4,8}, DIM in {2,3,4}, 16^2..16^4 incl. 4x16^3, "
-                               f"BETA in [2,4]*NC^2/3, {nsteps} MD steps/trajectory, DT tuned per chain, "
-                               "1 step = 1 trajectory of every chain",
-                   "chains": len(chains), "links_total": work // nsteps},
+        "config": {"workload": workload, "chains": len(chains), "links_total": work // nsteps},
         "alone_fp64": alone["fp64"], "alone_fp32": alone["fp32"],
         "batched_over_alone_fp64": batched / alone["fp64"],
         "batched_over_alone_fp32": batched / alone["fp32"],
@@ -653,7 +668,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="su3_32", choices=sorted(CONFIGS) + ["batch64"])
+    ap.add_argument("--config", default="su3_32", choices=sorted(CONFIGS) + ["batch64", "batch_su3_32"])
     ap.add_argument("--cpu-md-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-precision", action="store_true")
@@ -667,7 +682,7 @@ def main():
         line = run_kernel_only(args)
     elif args.impl == "reference":
         line = run_reference(args)
-    elif args.config == "batch64":
+    elif args.config in ("batch64", "batch_su3_32"):
         line = run_batch(args)
     else:
         line = run_ours(args)
