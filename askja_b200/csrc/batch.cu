@@ -145,6 +145,8 @@ cudaError_t launch_force(askja_batch* b, const askja_batch::Group& g, cudaStream
 #define ROWS(NM)                                                                                              \
   if (g.nmax == NM) {                                                                                         \
     auto k = mode ? kb_force_rows<NM, T, 1> : kb_force_rows<NM, T, 0>;                                        \
+    if constexpr (sizeof(T) == 4 && NM == 8)                                                                  \
+      if (mode) k = kb_force_rows8f;                                                                          \
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.smem);                        \
     k<<<grid, blk, g.smem, st>>>(b->d_desc, g.d_start, g.d_ids, (int)g.chains.size(), b->cur, ks);          \
   }

@@ -124,6 +124,23 @@ __global__ void kb_force_rows(const ChainDev* __restrict__ descs, const int* __r
                                       item % sd.lat.D, (item / sd.lat.D) * G, smem_raw, piv_s, det_s);
 }
 
+// FP32 with NMAX = 8, fused kick + drift: at most 128 registers (four
+// 128-thread CTAs per SM), as the single-chain rows::k_force8.
+static __global__ void __launch_bounds__(256, 2) kb_force_rows8f(const ChainDev* __restrict__ descs,
+                                                          const int* __restrict__ item_start,
+                                                          const int* __restrict__ chain_ids, int nchains, int cur,
+                                                          double kick_scale) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ int piv_s[64];
+  __shared__ cpx<float> det_s[64];
+  __shared__ ChainDev sd;
+  const int item = load_chain(sd, descs, item_start, chain_ids, nchains);
+  const int G = blockDim.x / sd.lat.N;
+  rows::force_rows<8, float, float2, 1>(sd.lat, (const float2*)sd.U[cur], (const float2*)sd.P, (float2*)sd.P,
+                                        (float2*)sd.U[cur ^ 1], (float)(kick_scale * sd.dt), (float)sd.dt, sd.order,
+                                        sd.reunit, item % sd.lat.D, (item / sd.lat.D) * G, smem_raw, piv_s, det_s);
+}
+
 // Plaquette sums: item = RED_THREADS-site block; partial per chain block.
 template <typename S2>
 __global__ void __launch_bounds__(misc::RED_THREADS) kb_plaq(const ChainDev* __restrict__ descs,
