@@ -28,7 +28,8 @@ EXE_PATH = os.path.join(HERE, "askja")
 ASKJA_OK = 0
 ERRORS = {-1: "ASKJA_ERR_ARG", -2: "ASKJA_ERR_CUDA", -3: "ASKJA_ERR_IO", -4: "ASKJA_ERR_NONFINITE",
           -5: "ASKJA_ERR_NODEVICE", -6: "ASKJA_ERR_PARSE"}
-FP64, FP32 = 0, 1
+FP64, FP32, FP32_LEAN = 0, 1, 2
+PRECISIONS = {"fp64": FP64, "fp32": FP32, "fp32-lean": FP32_LEAN}
 MAX_DIM = 16
 
 # every entry point include/askja_gpu.h declares
@@ -41,7 +42,7 @@ EXPORTS = [
     "askja_GaussLaw", "askja_UViol", "askja_WilsonLoop", "askja_PolyakovLoop", "askja_WilsonLoopDir",
     "askja_PlaqExp", "askja_scalarLoopcorr", "askja_eigenphases", "askja_trajectory", "askja_run_trajectories", "askja_leapfrog",
     "askja_md_steps", "askja_params_load", "askja_params_store", "askja_file_stem", "askja_conf_write",
-    "askja_conf_read", "askja_host_alloc", "askja_host_free", "askja_plaqexp_static", "askja_peak_flops",
+    "askja_conf_read", "askja_host_alloc", "askja_host_free", "askja_plaqexp_static",
     "askja_batch_create", "askja_batch_destroy", "askja_batch_last_error", "askja_batch_stream",
     "askja_batch_hot_start", "askja_batch_set_links", "askja_batch_get_links", "askja_batch_run",
     "askja_batch_plaquette", "askja_autotune", "askja_set_tuning", "askja_set_links_async", "askja_trajectory_async",
@@ -169,7 +170,7 @@ class Engine:
         for i, d in enumerate(dims):
             p.n[i] = d
         p.beta, p.dt, p.level = float(beta), float(dt), int(level)
-        p.precision = {"fp64": FP64, "fp32": FP32}[precision]
+        p.precision = PRECISIONS[precision]
         p.reunitarise = -1 if reunitarise is None else int(bool(reunitarise))
         p.device, p.kernel_path, p.seed = int(device), int(kernel_path), int(seed)
         self.params = p

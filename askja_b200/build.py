@@ -30,9 +30,12 @@ CXX = "g++"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
                   "--expt-relaxed-constexpr", "-ccbin", CXX]
-CU_SOURCES = ["kernels_fp64.cu", "kernels_fp32.cu", "engine.cu", "static_plaq.cu", "peak.cu", "batch.cu"]
+CU_SOURCES = ["kernels_fp64.cu", "kernels_fp32.cu", "kernels_split.cu", "engine.cu", "static_plaq.cu", "batch.cu"]
+# bench-only helper (compute-pipe peak probe for the roofline), not part of the product ABI
+PEAK_SRC = "peak.cu"
+PEAK_LIB = os.path.join(HERE, "libaskja_peak.so")
 CPP_SOURCES = ["hostio.cpp"]
-HEADERS = ["common.cuh", "small.cuh", "rows.cuh", "misc.cuh", "kernels.cuh", "launch.h", "batch.cuh", "tc.cuh", "eig.cuh", "pair.cuh", "tab.cuh"]
+HEADERS = ["common.cuh", "small.cuh", "rows.cuh", "misc.cuh", "kernels.cuh", "launch.h", "batch.cuh", "tc.cuh", "eig.cuh", "pair.cuh", "tab.cuh", "split.cuh", "split.h"]
 
 
 def _newer(target: str, deps) -> bool:
@@ -81,6 +84,9 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
     if _newer(LIB, objs):
         cmd = [NVCC] + ARCH + ["-shared", "-ccbin", CXX, "-o", LIB] + objs + ["-cudart", "static"]
         subprocess.check_call(cmd)
+    peak_src = os.path.join(CSRC, PEAK_SRC)
+    if _newer(PEAK_LIB, [peak_src]):
+        subprocess.check_call([NVCC] + NVFLAGS + ["-shared", peak_src, "-o", PEAK_LIB, "-cudart", "static"])
     libdir = os.path.dirname(LIB)
     for src, exe in (("askja_main.cpp", EXE), ("measure4d_main.cpp", MEASURE)):
         main_src = os.path.join(CSRC, src)

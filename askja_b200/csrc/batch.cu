@@ -20,6 +20,7 @@
 
 #include "../../include/askja_gpu.h"
 #include "batch.cuh"
+#include "launch.h"
 #include "kernels.cuh"
 
 using askja::Lat;
@@ -243,7 +244,7 @@ void* askja_batch_stream(askja_batch* b) { return b ? (void*)b->stream : nullptr
 
 void askja_batch_destroy(askja_batch* b) {
   if (!b) return;
-  cudaSetDevice(b->device);
+  askja::DevGuard g(b->device);
   if (b->stream) cudaStreamSynchronize(b->stream);
   drop_graphs(b);
   for (void* p : b->allocs) cudaFree(p);
@@ -273,7 +274,7 @@ int askja_batch_create(const askja_chain_params* chains, int nchains, int precis
     }
     if (V > (1L << 30)) return berr(nullptr, ASKJA_ERR_ARG, "chain %d: volume too large", c);
   }
-  cudaSetDevice(device);
+  askja::DevGuard g(device);
   b = new askja_batch();
   b->nchains = nchains;
   b->precision = precision;
@@ -409,7 +410,7 @@ int askja_batch_create(const askja_chain_params* chains, int nchains, int precis
 
 int askja_batch_hot_start(askja_batch* b, uint64_t seed) {
   if (int rc = check_chain(b, 0)) return rc;
-  cudaSetDevice(b->device);
+  askja::DevGuard g(b->device);
   for (int c = 0; c < b->nchains; c++) {
     askja::LaunchCtx lc = chain_lc(b, c);
     ChainDev& d = b->desc[c];
@@ -425,7 +426,7 @@ int askja_batch_hot_start(askja_batch* b, uint64_t seed) {
 int askja_batch_set_links(askja_batch* b, int c, const double* conf) {
   if (int rc = check_chain(b, c)) return rc;
   if (!conf) return berr(b, ASKJA_ERR_ARG, "null buffer");
-  cudaSetDevice(b->device);
+  askja::DevGuard g(b->device);
   ChainDev& d = b->desc[c];
   const size_t bytes = (size_t)d.lat.V * d.lat.D * d.lat.N * d.lat.N * 16;
   for (size_t i = 0; i < bytes / 8; i++)
@@ -441,7 +442,7 @@ int askja_batch_set_links(askja_batch* b, int c, const double* conf) {
 int askja_batch_get_links(askja_batch* b, int c, double* conf) {
   if (int rc = check_chain(b, c)) return rc;
   if (!conf) return berr(b, ASKJA_ERR_ARG, "null buffer");
-  cudaSetDevice(b->device);
+  askja::DevGuard g(b->device);
   ChainDev& d = b->desc[c];
   const size_t bytes = (size_t)d.lat.V * d.lat.D * d.lat.N * d.lat.N * 16;
   askja::LaunchCtx lc = chain_lc(b, c);
@@ -454,7 +455,7 @@ int askja_batch_get_links(askja_batch* b, int c, double* conf) {
 int askja_batch_run(askja_batch* b, int ntraj, int nsteps, int use_graph, askja_traj_result* results) {
   if (int rc = check_chain(b, 0)) return rc;
   if (ntraj < 0 || nsteps < 1) return berr(b, ASKJA_ERR_ARG, "bad trajectory counts");
-  cudaSetDevice(b->device);
+  askja::DevGuard g(b->device);
   for (int t = 0; t < ntraj; t++) {
     if (!use_graph) {
       if (int rc = enqueue(b, nsteps)) return rc;
@@ -489,7 +490,7 @@ int askja_batch_run(askja_batch* b, int ntraj, int nsteps, int use_graph, askja_
 int askja_batch_plaquette(askja_batch* b, double* out) {
   if (int rc = check_chain(b, 0)) return rc;
   if (!out) return berr(b, ASKJA_ERR_ARG, "null output");
-  cudaSetDevice(b->device);
+  askja::DevGuard g(b->device);
   int rc = b->precision == ASKJA_FP64 ? energies<double>(b, 2) : energies<float>(b, 2);
   if (rc) return rc;
   BCK(cudaStreamSynchronize(b->stream));

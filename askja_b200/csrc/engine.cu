@@ -25,7 +25,9 @@
 #include "../../include/askja_gpu.h"
 #include "launch.h"
 #include "misc.cuh"
+#include "split.h"
 
+using askja::DevGuard;
 using askja::KernelSet;
 using askja::Lat;
 using askja::LaunchCtx;
@@ -77,6 +79,19 @@ struct askja_ctx {
   unsigned long long* up_bad = nullptr;
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
   int g_nsteps[2] = {-1, -1};
+  // residual-plane FP32 mode (ASKJA_FP32, NC <= 4, thread per link; split.h):
+  // bfloat16 residuals of the links (UL, ULconf; lo_bytes each) and the
+  // momenta pi / Pi as FP32 coordinates (PC, P2C; coef_bytes) plus residuals
+  // (PCL, P2CL; coefl_bytes).  P and P2 then hold full FP32 matrices made from
+  // the coordinates on demand, for the matrix diagnostics (Gauss law, Tab).
+  bool split = false;
+  void* UL[2] = {nullptr, nullptr};
+  void* ULconf = nullptr;
+  void* PC = nullptr;
+  void* PCL = nullptr;
+  void* P2C = nullptr;
+  void* P2CL = nullptr;
+  size_t lo_bytes = 0, coef_bytes = 0, coefl_bytes = 0;
   std::string err;
 };
 
@@ -101,9 +116,6 @@ int set_err(askja_ctx* c, int code, const char* fmt, ...) {
     if (e_ != cudaSuccess) return set_err(c, ASKJA_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
   } while (0)
 
-struct DevGuard {
-  explicit DevGuard(int dev) { cudaSetDevice(dev); }
-};
 
 // neighbour tables from the reference's coordinate scheme (structs.h:169-218)
 void build_neighbours(const askja_params& p, long V, std::vector<int>& nbr) {
@@ -136,6 +148,78 @@ int check_ctx(askja_ctx* c) {
 }
 
 void* cur_u(askja_ctx* c) { return c->U[c->cur]; }
+void* cur_ul(askja_ctx* c) { return c->UL[c->cur]; }
+
+// Uconf <- U (save) or U <- Uconf (restore), residual planes included
+cudaError_t copy_saved(askja_ctx* c, bool save) {
+  void* d = save ? c->Uconf : cur_u(c);
+  const void* src = save ? cur_u(c) : c->Uconf;
+  cudaError_t e = cudaMemcpyAsync(d, src, c->field_bytes, cudaMemcpyDeviceToDevice, c->stream);
+  if (e == cudaSuccess && c->split)
+    e = cudaMemcpyAsync(save ? c->ULconf : cur_ul(c), save ? cur_ul(c) : c->ULconf, c->lo_bytes,
+                        cudaMemcpyDeviceToDevice, c->stream);
+  return e;
+}
+
+// pi <- Pi (the copy in updateUandcopyDown)
+cudaError_t copy_down(askja_ctx* c) {
+  if (!c->split) return cudaMemcpyAsync(c->P, c->P2, c->field_bytes, cudaMemcpyDeviceToDevice, c->stream);
+  cudaError_t e = cudaMemcpyAsync(c->PC, c->P2C, c->coef_bytes, cudaMemcpyDeviceToDevice, c->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(c->PCL, c->P2CL, c->coefl_bytes, cudaMemcpyDeviceToDevice, c->stream);
+  return e;
+}
+
+// the kick (mode 0) or fused kick + drift (mode 1) on pi (which 0) or Pi (1)
+// into pi / Pi, links into the partner buffer (mode 1)
+cudaError_t force_launch(askja_ctx* c, int mode, int in, int out, double ek, double ed) {
+  if (c->split) {
+    void* Uo = mode == 1 ? c->U[1 - c->cur] : nullptr;
+    void* ULo = mode == 1 ? c->UL[1 - c->cur] : nullptr;
+    return askja::splitk::force(c->lc, mode, cur_u(c), cur_ul(c), in ? c->P2C : c->PC, in ? c->P2CL : c->PCL,
+                                out ? c->P2C : c->PC, out ? c->P2CL : c->PCL, Uo, ULo, ek, ed);
+  }
+  return c->ks->force(c->lc, mode, cur_u(c), in ? c->P2 : c->P, out ? c->P2 : c->P,
+                      mode == 1 ? c->U[1 - c->cur] : nullptr, ek, ed);
+}
+
+// U <- exp(i eps Pi) U in place (updateUandcopyDown before its copy)
+cudaError_t drift_launch(askja_ctx* c, double eps) {
+  if (c->split) return askja::splitk::drift(c->lc, cur_u(c), cur_ul(c), c->P2C, c->P2CL, eps);
+  return c->ks->drift(c->lc, cur_u(c), c->P2, eps);
+}
+
+cudaError_t plaq_launch(askja_ctx* c) {
+  if (c->split) return askja::splitk::plaq(c->lc, cur_u(c), cur_ul(c), c->partial, c->sums);
+  return c->ks->plaq(c->lc, cur_u(c), c->partial, c->sums);
+}
+
+// link sums into sums[2..4]: Pa / Pb = 0 pi, 1 Pi, -1 none
+cudaError_t linksums_launch(askja_ctx* c, int pa, int pb, bool with_u) {
+  if (c->split) {
+    auto hi = [&](int w) -> const void* { return w < 0 ? nullptr : w ? c->P2C : c->PC; };
+    auto lo = [&](int w) -> const void* { return w < 0 ? nullptr : w ? c->P2CL : c->PCL; };
+    return askja::splitk::linksums(c->lc, hi(pa), lo(pa), hi(pb), lo(pb), with_u ? cur_u(c) : nullptr,
+                                   with_u ? cur_ul(c) : nullptr, c->partial, c->sums + 2);
+  }
+  auto m = [&](int w) -> const void* { return w < 0 ? nullptr : w ? c->P2 : c->P; };
+  return c->ks->linksums(c->lc, m(pa), m(pb), with_u ? cur_u(c) : nullptr, c->partial, c->sums + 2);
+}
+
+cudaError_t refresh_launch(askja_ctx* c, uint64_t seed, const unsigned long long* traj_dev,
+                           unsigned long long traj_host) {
+  const double scale = std::sqrt(2.0 * c->N / c->p.beta);
+  if (c->split) return askja::splitk::refresh(c->lc, c->PC, c->PCL, seed, traj_dev, traj_host, scale);
+  return c->ks->refresh(c->lc, c->P, seed, traj_dev, traj_host, scale);
+}
+
+// full FP32 matrices of pi and Pi in P / P2 (residual-plane mode) for the
+// kernels that read momentum matrices
+cudaError_t momenta_views(askja_ctx* c) {
+  if (!c->split) return cudaSuccess;
+  cudaError_t e = askja::splitk::momenta_to_matrix(c->lc, c->PC, c->PCL, c->P);
+  if (e == cudaSuccess) e = askja::splitk::momenta_to_matrix(c->lc, c->P2C, c->P2CL, c->P2);
+  return e;
+}
 
 int launch_ok(askja_ctx* c, cudaError_t e, const char* what) {
   if (e != cudaSuccess) return set_err(c, ASKJA_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
@@ -170,7 +254,7 @@ int fused_steps(askja_ctx* c, int n, double first_kick, double dt) {
   if (n <= 0) return ASKJA_OK;
   if (int rc = pair_layout(c, c->P)) return rc;
   for (int i = 0; i < n; i++) {
-    KL(c->ks->force(c->lc, 1, cur_u(c), c->P, c->P, c->U[1 - c->cur], i == 0 ? first_kick : dt, dt), "kick+drift");
+    KL(force_launch(c, 1, 0, 0, i == 0 ? first_kick : dt, dt), "kick+drift");
     c->cur ^= 1;
   }
   return pair_layout(c, c->P);
@@ -179,8 +263,13 @@ int fused_steps(askja_ctx* c, int n, double first_kick, double dt) {
 // Enqueue one whole trajectory (no host synchronisation; graph-capturable).
 int enqueue_trajectory(askja_ctx* c, int nsteps) {
   const double dt = c->p.dt;
-  const double scale = std::sqrt(2.0 * c->N / c->p.beta);
-  if (c->lc.reunit && (c->lc.force_rows == 2 || (c->lc.rows_ns && uses_rows(c)))) {
+  if (c->split && c->lc.reunit) {
+    // residual-plane mode: the link updates are not projected; every
+    // trajectory starts from links projected onto SU(N) in FP64 (the saved
+    // copy follows, so a rejected trajectory restores projected links)
+    KL(askja::splitk::reunit(c->lc, cur_u(c), cur_ul(c)), "reunitarise");
+    KL(copy_saved(c, true), "save links");
+  } else if (c->lc.reunit && (c->lc.force_rows == 2 || (c->lc.rows_ns && uses_rows(c)))) {
     // the tensor-core link update keeps U' exactly as unitary as U (it
     // projects exp(i eps P), not U'); the rounding defect U accumulates (an
     // unbiased random walk, ~6e-8 sqrt(MD steps)) is removed here, before
@@ -193,19 +282,22 @@ int enqueue_trajectory(askja_ctx* c, int nsteps) {
     KL(c->ks->reunit(lc, cur_u(c)), "reunitarise");
     KL(cudaMemcpyAsync(c->Uconf, cur_u(c), c->field_bytes, cudaMemcpyDeviceToDevice, c->stream), "save links");
   }
-  KL(c->ks->refresh(c->lc, c->P, c->p.seed, &c->st->traj, 0, scale), "refresh");
-  KL(c->ks->plaq(c->lc, cur_u(c), c->partial, c->sums), "plaq");
-  KL(c->ks->linksums(c->lc, c->P, nullptr, nullptr, c->partial, c->sums + 2), "kinetic");
+  KL(refresh_launch(c, c->p.seed, &c->st->traj, 0), "refresh");
+  KL(plaq_launch(c), "plaq");
+  KL(linksums_launch(c, 0, -1, false), "kinetic");
   askja::misc::k_energy<<<1, 1, 0, c->stream>>>(c->sums, c->p.beta, c->N, &c->st->h_old);
   KL(cudaGetLastError(), "energy");
   if (int rc = fused_steps(c, nsteps, 0.5 * dt, dt)) return rc;
-  KL(c->ks->force(c->lc, 0, cur_u(c), c->P, c->P, nullptr, 0.5 * dt, 0.0), "kick");
-  KL(c->ks->plaq(c->lc, cur_u(c), c->partial, c->sums), "plaq");
-  KL(c->ks->linksums(c->lc, c->P, nullptr, nullptr, c->partial, c->sums + 2), "kinetic");
+  KL(force_launch(c, 0, 0, 0, 0.5 * dt, 0.0), "kick");
+  KL(plaq_launch(c), "plaq");
+  KL(linksums_launch(c, 0, -1, false), "kinetic");
   askja::misc::k_energy<<<1, 1, 0, c->stream>>>(c->sums, c->p.beta, c->N, &c->st->h_new);
   askja::misc::k_metropolis<<<1, 1, 0, c->stream>>>(c->st, c->p.seed, c->logbuf, c->logcap);
   askja::misc::k_accept_copy<<<4 * 148, 256, 0, c->stream>>>(c->st, (uint4*)cur_u(c), (uint4*)c->Uconf,
                                                              (long)(c->field_bytes / 16));
+  if (c->split)
+    askja::misc::k_accept_copy<<<4 * 148, 256, 0, c->stream>>>(c->st, (uint4*)cur_ul(c), (uint4*)c->ULconf,
+                                                               (long)(c->lo_bytes / 16));
   KL(cudaGetLastError(), "metropolis");
   return ASKJA_OK;
 }
@@ -241,13 +333,48 @@ int sync_checked(askja_ctx* c) {
   return ASKJA_OK;
 }
 
+// kind of a device field for the conversions: the links (current or saved) or a momentum buffer
+enum class FieldKind { links, saved_links, pi, Pi };
+
+// U-conf layout (FP64) -> device field; in the residual-plane mode `dst` is
+// ignored and the kind picks the hi/lo (links) or coordinate (momenta) buffers
+cudaError_t from_conf_launch(askja_ctx* c, const void* conf, void* dst, FieldKind kind) {
+  if (!c->split) return c->ks->from_conf(c->lc, conf, dst);
+  switch (kind) {
+    case FieldKind::links:
+      return askja::splitk::links_from_conf(c->lc, conf, cur_u(c), cur_ul(c));
+    case FieldKind::saved_links:
+      return askja::splitk::links_from_conf(c->lc, conf, c->Uconf, c->ULconf);
+    case FieldKind::pi:
+      return askja::splitk::momenta_from_conf(c->lc, conf, c->PC, c->PCL);
+    case FieldKind::Pi:
+      return askja::splitk::momenta_from_conf(c->lc, conf, c->P2C, c->P2CL);
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t to_conf_launch(askja_ctx* c, const void* src, void* conf, FieldKind kind) {
+  if (!c->split) return c->ks->to_conf(c->lc, src, conf);
+  switch (kind) {
+    case FieldKind::links:
+      return askja::splitk::links_to_conf(c->lc, cur_u(c), cur_ul(c), conf);
+    case FieldKind::saved_links:
+      return askja::splitk::links_to_conf(c->lc, c->Uconf, c->ULconf, conf);
+    case FieldKind::pi:
+      return askja::splitk::momenta_to_conf(c->lc, c->PC, c->PCL, conf);
+    case FieldKind::Pi:
+      return askja::splitk::momenta_to_conf(c->lc, c->P2C, c->P2CL, conf);
+  }
+  return cudaErrorInvalidValue;
+}
+
 int read_state(askja_ctx* c, askja_traj_result* out) {
   if (!out) return sync_checked(c);
   CK(cudaMemcpyAsync(out, c->st, sizeof(TrajState), cudaMemcpyDeviceToHost, c->stream));
   return sync_checked(c);
 }
 
-int upload_conf(askja_ctx* c, const double* conf, void* dst) {
+int upload_conf(askja_ctx* c, const double* conf, void* dst, FieldKind kind = FieldKind::links) {
   const size_t bytes = (size_t)c->nl * c->N * c->N * 2 * sizeof(double);
   CK(cudaMemcpyAsync(c->staging, conf, bytes, cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemsetAsync(c->nonfinite, 0, sizeof(unsigned long long), c->stream));
@@ -257,13 +384,13 @@ int upload_conf(askja_ctx* c, const double* conf, void* dst) {
   CK(cudaMemcpyAsync(&bad, c->nonfinite, sizeof bad, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   if (bad) return set_err(c, ASKJA_ERR_NONFINITE, "input buffer holds %llu non-finite values", bad);
-  KL(c->ks->from_conf(c->lc, c->staging, dst), "from_conf");
+  KL(from_conf_launch(c, c->staging, dst, kind), "from_conf");
   return ASKJA_OK;
 }
 
-int download_conf(askja_ctx* c, const void* src, double* conf) {
+int download_conf(askja_ctx* c, const void* src, double* conf, FieldKind kind = FieldKind::links) {
   const size_t bytes = (size_t)c->nl * c->N * c->N * 2 * sizeof(double);
-  KL(c->ks->to_conf(c->lc, src, c->staging), "to_conf");
+  KL(to_conf_launch(c, src, c->staging, kind), "to_conf");
   CK(cudaMemcpyAsync(conf, c->staging, bytes, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return ASKJA_OK;
@@ -293,7 +420,7 @@ int askja_sync(askja_ctx* c) {
 
 void askja_destroy(askja_ctx* c) {
   if (!c) return;
-  cudaSetDevice(c->p.device);
+  DevGuard g(c->p.device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
   drop_graphs(c);
@@ -304,8 +431,9 @@ void askja_destroy(askja_ctx* c) {
   }
   if (c->up_bad) cudaFree(c->up_bad);
   if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
-  void* bufs[] = {c->U[0], c->U[1], c->P, c->P2, c->Uconf, c->nbr, c->partial, c->sums, c->lines,
-                  c->st,   c->logbuf, c->staging, c->nonfinite, c->tc_status, c->eigs, c->eigfail};
+  void* bufs[] = {c->U[0], c->U[1], c->P,      c->P2,      c->Uconf,     c->nbr,       c->partial, c->sums,
+                  c->lines, c->st,  c->logbuf, c->staging, c->nonfinite, c->tc_status, c->eigs,    c->eigfail,
+                  c->UL[0], c->UL[1], c->ULconf, c->PC, c->PCL, c->P2C, c->P2CL};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -326,7 +454,7 @@ int askja_create(const askja_params* p, askja_ctx** out) {
     if (V > (1L << 30)) return set_err(nullptr, ASKJA_ERR_ARG, "volume too large");
   }
   if (!(p->beta > 0.0) || !std::isfinite(p->beta)) return set_err(nullptr, ASKJA_ERR_ARG, "BETA must be > 0");
-  if (p->precision != ASKJA_FP64 && p->precision != ASKJA_FP32)
+  if (p->precision != ASKJA_FP64 && p->precision != ASKJA_FP32 && p->precision != ASKJA_FP32_LEAN)
     return set_err(nullptr, ASKJA_ERR_ARG, "unknown precision %d", p->precision);
   if (p->kernel_path < 0 || p->kernel_path > 3)
     return set_err(nullptr, ASKJA_ERR_ARG, "unknown kernel path %d", p->kernel_path);
@@ -348,6 +476,8 @@ int askja_create(const askja_params* p, askja_ctx** out) {
   c->V = V;
   c->nl = V * p->dim;
   c->ks = p->precision == ASKJA_FP64 ? &askja::kernels_fp64 : &askja::kernels_fp32;
+  // residual planes: ASKJA_FP32 on the thread-per-link mapping (NC <= 4, automatic kernel path)
+  c->split = p->precision == ASKJA_FP32 && askja::splitk::supported(p->nc) && p->kernel_path == 0;
   const size_t elem = p->precision == ASKJA_FP64 ? 16 : 8;
   Lat& L = c->lat;
   L.V = (int)V;
@@ -394,6 +524,23 @@ int askja_create(const askja_params* p, askja_ctx** out) {
   CKC(cudaMalloc(&c->staging, (size_t)c->nl * c->N * c->N * 2 * sizeof(double)));
   CKC(cudaMalloc(&c->nonfinite, sizeof(unsigned long long)));
   for (void* b : {c->U[0], c->U[1], c->P, c->P2, c->Uconf}) CKC(cudaMemset(b, 0, c->field_bytes));
+  if (c->split) {
+    c->lo_bytes = askja::field_elems(L) * sizeof(uint32_t);
+    c->coef_bytes = askja::splitk::coef_floats(L) * sizeof(float);
+    c->coefl_bytes = askja::splitk::coef_words(L) * sizeof(uint32_t);
+    for (void** b : {&c->UL[0], &c->UL[1], &c->ULconf}) {
+      CKC(cudaMalloc(b, c->lo_bytes));
+      CKC(cudaMemset(*b, 0, c->lo_bytes));
+    }
+    for (void** b : {&c->PC, &c->P2C}) {
+      CKC(cudaMalloc(b, c->coef_bytes));
+      CKC(cudaMemset(*b, 0, c->coef_bytes));
+    }
+    for (void** b : {&c->PCL, &c->P2CL}) {
+      CKC(cudaMalloc(b, c->coefl_bytes));
+      CKC(cudaMemset(*b, 0, c->coefl_bytes));
+    }
+  }
   c->lc.lat = L;
   c->lc.stream = c->stream;
   c->lc.order = askja::taylor_order(p->level);
@@ -433,7 +580,7 @@ int askja_set_links(askja_ctx* c, const double* conf) {
   if (!conf) return set_err(c, ASKJA_ERR_ARG, "null buffer");
   DevGuard g(c->p.device);
   if (int rc = upload_conf(c, conf, cur_u(c))) return rc;
-  CK(cudaMemcpyAsync(c->Uconf, cur_u(c), c->field_bytes, cudaMemcpyDeviceToDevice, c->stream));
+  CK(copy_saved(c, true));
   CK(cudaStreamSynchronize(c->stream));
   return ASKJA_OK;
 }
@@ -465,8 +612,8 @@ int askja_set_links_async(askja_ctx* c, const double* conf) {
   askja::misc::k_count_nonfinite<<<4 * 148, 256, 0, c->stream>>>((const double*)c->up[b],
                                                                   (long)(bytes / sizeof(double)), c->up_bad);
   KL(cudaGetLastError(), "non-finite check");
-  KL(c->ks->from_conf(c->lc, c->up[b], cur_u(c)), "from_conf");
-  CK(cudaMemcpyAsync(c->Uconf, cur_u(c), c->field_bytes, cudaMemcpyDeviceToDevice, c->stream));
+  KL(from_conf_launch(c, c->up[b], cur_u(c), FieldKind::links), "from_conf");
+  CK(copy_saved(c, true));
   CK(cudaEventRecord(c->up_free[b], c->stream));
   return ASKJA_OK;
 }
@@ -482,14 +629,14 @@ int askja_get_saved_links(askja_ctx* c, double* conf) {
   if (int rc = check_ctx(c)) return rc;
   if (!conf) return set_err(c, ASKJA_ERR_ARG, "null buffer");
   DevGuard g(c->p.device);
-  return download_conf(c, c->Uconf, conf);
+  return download_conf(c, c->Uconf, conf, FieldKind::saved_links);
 }
 
 int askja_set_momenta(askja_ctx* c, int which, const double* conf) {
   if (int rc = check_ctx(c)) return rc;
   if (!conf || (which != 0 && which != 1)) return set_err(c, ASKJA_ERR_ARG, "bad momentum buffer selector");
   DevGuard g(c->p.device);
-  if (int rc = upload_conf(c, conf, which ? c->P2 : c->P)) return rc;
+  if (int rc = upload_conf(c, conf, which ? c->P2 : c->P, which ? FieldKind::Pi : FieldKind::pi)) return rc;
   CK(cudaStreamSynchronize(c->stream));
   return ASKJA_OK;
 }
@@ -498,14 +645,15 @@ int askja_get_momenta(askja_ctx* c, int which, double* conf) {
   if (int rc = check_ctx(c)) return rc;
   if (!conf || (which != 0 && which != 1)) return set_err(c, ASKJA_ERR_ARG, "bad momentum buffer selector");
   DevGuard g(c->p.device);
-  return download_conf(c, which ? c->P2 : c->P, conf);
+  return download_conf(c, which ? c->P2 : c->P, conf, which ? FieldKind::Pi : FieldKind::pi);
 }
 
 int askja_initializeU(askja_ctx* c) {
   if (int rc = check_ctx(c)) return rc;
   DevGuard g(c->p.device);
   KL(c->ks->identity(c->lc, cur_u(c)), "identity");
-  CK(cudaMemcpyAsync(c->Uconf, cur_u(c), c->field_bytes, cudaMemcpyDeviceToDevice, c->stream));
+  if (c->split) CK(cudaMemsetAsync(cur_ul(c), 0, c->lo_bytes, c->stream));
+  CK(copy_saved(c, true));
   CK(cudaStreamSynchronize(c->stream));
   return ASKJA_OK;
 }
@@ -515,9 +663,14 @@ int askja_hot_start(askja_ctx* c, uint64_t seed) {
   DevGuard g(c->p.device);
   KL(c->ks->gauss_matrices(c->lc, cur_u(c), seed), "gaussian matrices");
   // Gram-Schmidt + determinant phase always, whatever the reunitarise setting
-  LaunchCtx lc = c->lc;
-  KL(c->ks->reunit(lc, cur_u(c)), "reunitarise");
-  CK(cudaMemcpyAsync(c->Uconf, cur_u(c), c->field_bytes, cudaMemcpyDeviceToDevice, c->stream));
+  if (c->split) {
+    CK(cudaMemsetAsync(cur_ul(c), 0, c->lo_bytes, c->stream));
+    KL(askja::splitk::reunit(c->lc, cur_u(c), cur_ul(c)), "reunitarise");
+  } else {
+    LaunchCtx lc = c->lc;
+    KL(c->ks->reunit(lc, cur_u(c)), "reunitarise");
+  }
+  CK(copy_saved(c, true));
   CK(cudaStreamSynchronize(c->stream));
   return ASKJA_OK;
 }
@@ -525,8 +678,7 @@ int askja_hot_start(askja_ctx* c, uint64_t seed) {
 int askja_initializeE(askja_ctx* c, uint64_t seed, uint64_t counter) {
   if (int rc = check_ctx(c)) return rc;
   DevGuard g(c->p.device);
-  const double scale = std::sqrt(2.0 * c->N / c->p.beta);
-  KL(c->ks->refresh(c->lc, c->P, seed, nullptr, (unsigned long long)counter, scale), "refresh");
+  KL(refresh_launch(c, seed, nullptr, (unsigned long long)counter), "refresh");
   CK(cudaStreamSynchronize(c->stream));
   return ASKJA_OK;
 }
@@ -534,7 +686,7 @@ int askja_initializeE(askja_ctx* c, uint64_t seed, uint64_t counter) {
 int askja_updateE(askja_ctx* c, double eps) {
   if (int rc = check_ctx(c)) return rc;
   DevGuard g(c->p.device);
-  KL(c->ks->force(c->lc, 0, cur_u(c), c->P, c->P2, nullptr, eps, 0.0), "updateE");
+  KL(force_launch(c, 0, 0, 1, eps, 0.0), "updateE");
   CK(cudaStreamSynchronize(c->stream));
   return ASKJA_OK;
 }
@@ -542,8 +694,8 @@ int askja_updateE(askja_ctx* c, double eps) {
 int askja_updateUandcopyDown(askja_ctx* c, double eps) {
   if (int rc = check_ctx(c)) return rc;
   DevGuard g(c->p.device);
-  KL(c->ks->drift(c->lc, cur_u(c), c->P2, eps), "drift");
-  CK(cudaMemcpyAsync(c->P, c->P2, c->field_bytes, cudaMemcpyDeviceToDevice, c->stream));
+  KL(drift_launch(c, eps), "drift");
+  CK(copy_down(c));
   CK(cudaStreamSynchronize(c->stream));
   return ASKJA_OK;
 }
@@ -551,7 +703,7 @@ int askja_updateUandcopyDown(askja_ctx* c, double eps) {
 int askja_copyDown(askja_ctx* c) {
   if (int rc = check_ctx(c)) return rc;
   DevGuard g(c->p.device);
-  CK(cudaMemcpyAsync(c->P, c->P2, c->field_bytes, cudaMemcpyDeviceToDevice, c->stream));
+  CK(copy_down(c));
   CK(cudaStreamSynchronize(c->stream));
   return ASKJA_OK;
 }
@@ -559,7 +711,7 @@ int askja_copyDown(askja_ctx* c) {
 int askja_takeconfiguration(askja_ctx* c) {
   if (int rc = check_ctx(c)) return rc;
   DevGuard g(c->p.device);
-  CK(cudaMemcpyAsync(c->Uconf, cur_u(c), c->field_bytes, cudaMemcpyDeviceToDevice, c->stream));
+  CK(copy_saved(c, true));
   CK(cudaStreamSynchronize(c->stream));
   return ASKJA_OK;
 }
@@ -567,7 +719,7 @@ int askja_takeconfiguration(askja_ctx* c) {
 int askja_loadconfiguration(askja_ctx* c) {
   if (int rc = check_ctx(c)) return rc;
   DevGuard g(c->p.device);
-  CK(cudaMemcpyAsync(cur_u(c), c->Uconf, c->field_bytes, cudaMemcpyDeviceToDevice, c->stream));
+  CK(copy_saved(c, false));
   CK(cudaStreamSynchronize(c->stream));
   return ASKJA_OK;
 }
@@ -575,7 +727,10 @@ int askja_loadconfiguration(askja_ctx* c) {
 int askja_reunitarise(askja_ctx* c) {
   if (int rc = check_ctx(c)) return rc;
   DevGuard g(c->p.device);
-  KL(c->ks->reunit(c->lc, cur_u(c)), "reunitarise");
+  if (c->split)
+    KL(askja::splitk::reunit(c->lc, cur_u(c), cur_ul(c)), "reunitarise");
+  else
+    KL(c->ks->reunit(c->lc, cur_u(c)), "reunitarise");
   CK(cudaStreamSynchronize(c->stream));
   return ASKJA_OK;
 }
@@ -583,7 +738,7 @@ int askja_reunitarise(askja_ctx* c) {
 int askja_PlaqExp(askja_ctx* c, double* temporal, double* spatial) {
   if (int rc = check_ctx(c)) return rc;
   DevGuard g(c->p.device);
-  KL(c->ks->plaq(c->lc, cur_u(c), c->partial, c->sums), "plaq");
+  KL(plaq_launch(c), "plaq");
   double h[2];
   if (int rc = scal(c, c->sums, h, 2)) return rc;
   if (temporal) *temporal = h[0];
@@ -599,9 +754,10 @@ int askja_EnergyMag(askja_ctx* c, double* out) {
   return ASKJA_OK;
 }
 
-static int linksums(askja_ctx* c, const void* Pa, const void* Pb, const void* U, double h[3]) {
+// pa / pb: 0 pi, 1 Pi, -1 none
+static int linksums(askja_ctx* c, int pa, int pb, bool with_u, double h[3]) {
   DevGuard g(c->p.device);
-  KL(c->ks->linksums(c->lc, Pa, Pb, U, c->partial, c->sums + 2), "linksums");
+  KL(linksums_launch(c, pa, pb, with_u), "linksums");
   return scal(c, c->sums + 2, h, 3);
 }
 
@@ -609,7 +765,7 @@ int askja_simpleenergyEl(askja_ctx* c, int which, double* out) {
   if (int rc = check_ctx(c)) return rc;
   if (!out || (which != 0 && which != 1)) return set_err(c, ASKJA_ERR_ARG, "bad argument");
   double h[3];
-  if (int rc = linksums(c, which ? c->P2 : c->P, nullptr, nullptr, h)) return rc;
+  if (int rc = linksums(c, which, -1, false, h)) return rc;
   *out = h[0];
   return ASKJA_OK;
 }
@@ -618,7 +774,7 @@ int askja_EnergyEl(askja_ctx* c, double* out) {
   if (int rc = check_ctx(c)) return rc;
   if (!out) return set_err(c, ASKJA_ERR_ARG, "null output");
   double h[3];
-  if (int rc = linksums(c, c->P, c->P2, nullptr, h)) return rc;
+  if (int rc = linksums(c, 0, 1, false, h)) return rc;
   *out = h[1];
   return ASKJA_OK;
 }
@@ -627,7 +783,7 @@ int askja_UViol(askja_ctx* c, double* out) {
   if (int rc = check_ctx(c)) return rc;
   if (!out) return set_err(c, ASKJA_ERR_ARG, "null output");
   double h[3];
-  if (int rc = linksums(c, nullptr, nullptr, cur_u(c), h)) return rc;
+  if (int rc = linksums(c, -1, -1, true, h)) return rc;
   *out = h[2];
   return ASKJA_OK;
 }
@@ -645,6 +801,7 @@ int askja_GaussLaw(askja_ctx* c, double* out) {
   if (int rc = check_ctx(c)) return rc;
   if (!out) return set_err(c, ASKJA_ERR_ARG, "null output");
   DevGuard g(c->p.device);
+  KL(momenta_views(c), "momentum matrices");
   KL(c->ks->gauss(c->lc, cur_u(c), c->P2, c->partial, c->sums + 5), "gauss");
   return scal(c, c->sums + 5, out, 1);
 }
@@ -763,6 +920,7 @@ int askja_FourierTrafo(askja_ctx* c, double* coefficients) {
 static int tab_range(askja_ctx* c, long site0, long nsites, int npt, double* out_dev) {
   if (c->D > 8 || c->N > 64) return set_err(c, ASKJA_ERR_ARG, "Tab: DIM <= 8 and NC <= 64");
   if (npt < 2 || npt > c->D + 2) return set_err(c, ASKJA_ERR_ARG, "Tab: Npt must be in 2..DIM+2 (got %d)", npt);
+  KL(momenta_views(c), "momentum matrices");
   KL(c->ks->tab(c->lc, cur_u(c), c->P, c->P2, (int)site0, (int)nsites, npt, out_dev), "Tab");
   return ASKJA_OK;
 }
@@ -795,7 +953,7 @@ int askja_leapfrog(askja_ctx* c, int nsteps, double eps) {
   if (nsteps < 1) return set_err(c, ASKJA_ERR_ARG, "nsteps must be >= 1");
   DevGuard g(c->p.device);
   if (int rc = fused_steps(c, nsteps, 0.5 * eps, eps)) return rc;
-  KL(c->ks->force(c->lc, 0, cur_u(c), c->P, c->P, nullptr, 0.5 * eps, 0.0), "kick");
+  KL(force_launch(c, 0, 0, 0, 0.5 * eps, 0.0), "kick");
   CK(cudaStreamSynchronize(c->stream));
   return ASKJA_OK;
 }
@@ -806,12 +964,12 @@ int askja_md_steps(askja_ctx* c, int nsteps, double eps) {
   if (nsteps == 0) return ASKJA_OK;
   DevGuard g(c->p.device);
   // D(eps) with Pi, pi = Pi ...
-  KL(c->ks->drift(c->lc, cur_u(c), c->P2, eps), "drift");
-  CK(cudaMemcpyAsync(c->P, c->P2, c->field_bytes, cudaMemcpyDeviceToDevice, c->stream));
+  KL(drift_launch(c, eps), "drift");
+  CK(copy_down(c));
   // ... then (K D) fused, in place on pi ...
   if (int rc = fused_steps(c, nsteps - 1, eps, eps)) return rc;
   // ... and the last kick out of place: Pi = pi - eps F(u)
-  KL(c->ks->force(c->lc, 0, cur_u(c), c->P, c->P2, nullptr, eps, 0.0), "kick");
+  KL(force_launch(c, 0, 0, 1, eps, 0.0), "kick");
   CK(cudaStreamSynchronize(c->stream));
   return ASKJA_OK;
 }
@@ -894,7 +1052,7 @@ int askja_run_trajectories(askja_ctx* c, int ntraj, int nsteps, int use_graph, a
 
 int askja_set_tuning(askja_ctx* c, const askja_tuning* t) {
   if (int rc = check_ctx(c)) return rc;
-  if (!t || t->path < 0 || t->path > 3 || (t->path == 0 && c->N > 4) || t->groups < 0 ||
+  if (!t || t->path < 0 || t->path > 3 || (t->path == 0 && c->N > 4) || t->groups < 0 || (c->split && t->path != 0) ||
       (t->path == 2 && !askja::tc_supported(c->N, c->D, c->p.precision == ASKJA_FP64)) ||
       (t->path == 3 && !askja::pair_supported(c->N, c->D, c->p.precision == ASKJA_FP64, c->lat.n[c->D - 1])))
     return set_err(c, ASKJA_ERR_ARG, "invalid tuning");
@@ -922,7 +1080,9 @@ int askja_autotune(askja_ctx* c, int reps, askja_tuning* out) {
   if (askja::tc_supported(c->N, c->D, fp64)) cands.push_back({2, 0, 0});
 
   std::vector<int> seen;
+  // the residual-plane mode has one mapping (thread per link); only its register budget is tuned
   for (int want : {0, 2, 4, 8, 16, 32, 64}) {
+    if (c->split) break;
     const int eff = askja::rows_effective_groups(c->N, fp64, want);
     bool dup = false;
     for (int s : seen) dup |= s == eff;
@@ -933,6 +1093,16 @@ int askja_autotune(askja_ctx* c, int reps, askja_tuning* out) {
   if (cands.size() > 24) cands.resize(24);
   // scratch: Pi holds a copy of pi, the partner link buffer receives the output
   CK(cudaMemcpyAsync(c->P2, c->P, c->field_bytes, cudaMemcpyDeviceToDevice, c->stream));
+  if (c->split) {
+    CK(cudaMemcpyAsync(c->P2C, c->PC, c->coef_bytes, cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->P2CL, c->PCL, c->coefl_bytes, cudaMemcpyDeviceToDevice, c->stream));
+  }
+  auto fused = [&](const askja::LaunchCtx& lc) -> cudaError_t {
+    if (c->split)
+      return askja::splitk::force(lc, 1, cur_u(c), cur_ul(c), c->P2C, c->P2CL, c->P2C, c->P2CL, c->U[1 - c->cur],
+                                  c->UL[1 - c->cur], 0.5 * c->p.dt, c->p.dt);
+    return c->ks->force(lc, 1, cur_u(c), c->P2, c->P2, c->U[1 - c->cur], 0.5 * c->p.dt, c->p.dt);
+  };
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
@@ -950,11 +1120,9 @@ int askja_autotune(askja_ctx* c, int reps, askja_tuning* out) {
     cudaError_t e = cudaSuccess;
     if (pl) e = c->ks->pair_swap(lc, cur_u(c));
     if (pl && e == cudaSuccess) e = c->ks->pair_swap(lc, c->P2);
-    if (e == cudaSuccess)
-      e = c->ks->force(lc, 1, cur_u(c), c->P2, c->P2, c->U[1 - c->cur], 0.5 * c->p.dt, c->p.dt);
+    if (e == cudaSuccess) e = fused(lc);
     if (e == cudaSuccess) e = cudaEventRecord(e0, c->stream);
-    for (int r = 0; r < reps && e == cudaSuccess; r++)
-      e = c->ks->force(lc, 1, cur_u(c), c->P2, c->P2, c->U[1 - c->cur], 0.5 * c->p.dt, c->p.dt);
+    for (int r = 0; r < reps && e == cudaSuccess; r++) e = fused(lc);
     if (e == cudaSuccess) e = cudaEventRecord(e1, c->stream);
     if (pl && e == cudaSuccess) e = c->ks->pair_swap(lc, cur_u(c));
     if (pl && e == cudaSuccess) e = c->ks->pair_swap(lc, c->P2);

@@ -10,6 +10,23 @@
 
 namespace askja {
 
+// Makes `dev` current for the duration of one API call and gives the caller
+// back its own current device on return (every entry point that switches
+// devices uses it, so a caller working on another GPU keeps its device).
+struct DevGuard {
+  int prev = -1;
+  explicit DevGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DevGuard() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+  DevGuard(const DevGuard&) = delete;
+  DevGuard& operator=(const DevGuard&) = delete;
+};
+
 struct LaunchCtx {
   Lat lat;
   cudaStream_t stream;

@@ -287,13 +287,14 @@ __global__ void __launch_bounds__(RED_THREADS) k_slice_trace(Lat L, const S2* __
 // (i,j),(j,i); T_2p+1 has -i/2 at (i,j), +i/2 at (j,i); the m-th diagonal
 // generator is norm_m * diag(1,..,1 (m+1 times), -(m+1), 0, ..),
 // norm_m = sqrt(1 / (2 (m+1)(m+2))).
-template <typename S2>
-__device__ __forceinline__ void refresh_link(const Lat& L, S2* __restrict__ P, uint64_t seed, uint32_t traj,
-                                             double scale, long t) {
-  if (t >= (long)L.V * L.D) return;
+// The entries of one link's momentum in generation order: emit(i, j, value)
+// for the upper and lower entry of every off-diagonal pair, then the diagonal
+// from the last row up.  Shared by the matrix refresh below and the refresh of
+// the residual-plane FP32 mode (split.cuh), so both draw identical momenta.
+template <typename Emit>
+__device__ __forceinline__ void refresh_entries(const Lat& L, uint64_t seed, uint32_t traj, double scale, int d, int s,
+                                                Emit&& emit) {
   const int N = L.N;
-  const int d = (int)(t / L.V);
-  const int s = (int)(t - (long)d * L.V);
   const unsigned long long lk = (unsigned long long)s * L.D + d;
   const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
   int cur_blk = -1;
@@ -315,10 +316,8 @@ __device__ __forceinline__ void refresh_link(const Lat& L, S2* __restrict__ P, u
   for (int i = 0; i < N; i++)
     for (int j = i + 1; j < N; j++, p++) {
       const double xs = normal(2 * p), xa = normal(2 * p + 1);
-      cpx<double> a = mkc<double>(0.5 * scale * xs, -0.5 * scale * xa);
-      cpx<double> b = mkc<double>(0.5 * scale * xs, 0.5 * scale * xa);
-      stc(P + eoff(L, d, i * N + j, s), a);
-      stc(P + eoff(L, d, j * N + i, s), b);
+      emit(i, j, mkc<double>(0.5 * scale * xs, -0.5 * scale * xa));
+      emit(j, i, mkc<double>(0.5 * scale * xs, 0.5 * scale * xa));
     }
   // diagonal: P_dd = scale * (S_d - d * norm_{d-1} xi_{d-1}),  S_d = sum_{m>=d} norm_m xi_m
   const int a0 = N * (N - 1);
@@ -332,8 +331,19 @@ __device__ __forceinline__ void refresh_link(const Lat& L, S2* __restrict__ P, u
       val -= dd * nm * xm;
       suffix += nm * xm;
     }
-    stc(P + eoff(L, d, dd * N + dd, s), mkc<double>(scale * val, 0.0));
+    emit(dd, dd, mkc<double>(scale * val, 0.0));
   }
+}
+
+template <typename S2>
+__device__ __forceinline__ void refresh_link(const Lat& L, S2* __restrict__ P, uint64_t seed, uint32_t traj,
+                                             double scale, long t) {
+  if (t >= (long)L.V * L.D) return;
+  const int N = L.N;
+  const int d = (int)(t / L.V);
+  const int s = (int)(t - (long)d * L.V);
+  refresh_entries(L, seed, traj, scale, d, s,
+                  [&](int i, int j, const cpx<double>& v) { stc(P + eoff(L, d, i * N + j, s), v); });
 }
 
 template <typename S2>

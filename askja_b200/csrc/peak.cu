@@ -1,4 +1,5 @@
-// Compute-pipe peaks measured on the running GPU, for the compute side of the
+// Bench-only helper library (libaskja_peak.so, not part of the askja ABI):
+// compute-pipe peaks measured on the running GPU, for the compute side of the
 // roofline (the HBM and tensor peaks come from the pool's measured copy and
 // cuBLAS figures).  Each kernel runs long chains of independent fused
 // multiply-adds from registers: FP32 FFMA, FP32 packed FFMA2 (two lanes per
@@ -6,7 +7,9 @@
 // thread to keep the chains alive.
 #include <cuda_runtime.h>
 
-#include "../../include/askja_gpu.h"
+// status codes: 0 success, -1 bad argument, -2 a CUDA call failed
+constexpr int kOk = 0, kErrArg = -1, kErrCuda = -2;
+
 
 namespace {
 
@@ -57,14 +60,14 @@ __global__ void k_dfma(double* out, double a, double b) {
 
 // which: 0 = FFMA, 1 = FFMA2, 2 = DFMA.  Returns GFLOP/s (2 flops per FMA
 // lane) in *gflops, best of `repeats` timed launches.
-extern "C" ASKJA_API int askja_peak_flops(int device, int which, int repeats, double* gflops) {
-  if (!gflops || which < 0 || which > 2 || repeats < 1) return ASKJA_ERR_ARG;
-  if (cudaSetDevice(device) != cudaSuccess) return ASKJA_ERR_CUDA;
+extern "C" __attribute__((visibility("default"))) int askja_peak_flops(int device, int which, int repeats, double* gflops) {
+  if (!gflops || which < 0 || which > 2 || repeats < 1) return kErrArg;
+  if (cudaSetDevice(device) != cudaSuccess) return kErrCuda;
   int sms = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   const int threads = 256, blocks = sms * 8;
   void* out = nullptr;
-  if (cudaMalloc(&out, (size_t)threads * blocks * sizeof(double)) != cudaSuccess) return ASKJA_ERR_CUDA;
+  if (cudaMalloc(&out, (size_t)threads * blocks * sizeof(double)) != cudaSuccess) return kErrCuda;
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
@@ -84,9 +87,9 @@ extern "C" ASKJA_API int askja_peak_flops(int device, int which, int repeats, do
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   cudaFree(out);
-  if (err != cudaSuccess) return ASKJA_ERR_CUDA;
+  if (err != cudaSuccess) return kErrCuda;
   const double lanes = which == 1 ? 2.0 : 1.0;
   const double fmas = (double)threads * blocks * kIters * kChains * lanes;
   *gflops = 2.0 * fmas / (best * 1e-3) / 1e9;
-  return ASKJA_OK;
+  return kOk;
 }

@@ -24,6 +24,7 @@
 
 #include "../../include/askja_gpu.h"
 #include "common.cuh"
+#include "launch.h"
 #include "misc.cuh"
 
 namespace {
@@ -157,7 +158,11 @@ extern "C" int askja_plaqexp_static(const askja_params* p, const void* links, do
     askja_internal_set_error("askja_plaqexp_static: device not present");
     return ASKJA_ERR_ARG;
   }
-  cudaError_t e = cudaSetDevice(p->device);
+  // the caller's current device is restored on return
+  askja::DevGuard guard(p->device);
+  int cur = -1;
+  cudaError_t e = cudaGetDevice(&cur);
+  if (e == cudaSuccess && cur != p->device) e = cudaErrorInvalidDevice;
   double* scratch = nullptr;
   if (e == cudaSuccess) {
     if (int rc = scratch_for(p->device, &scratch, msg, sizeof msg)) {

@@ -51,6 +51,21 @@ CONFIGS = {
                       cpu_dims=[2, 2, 4], ensemble=20),
 }
 
+BATCH_CONFIGS = ("batch64", "batch_su3_32")
+
+
+def metric_for(config: str) -> str:
+    """The metric string of a workload, identical in both arms (ours and
+    --impl reference) so that their values can be divided."""
+    if config == "batch_su3_32":
+        return "link-updates/s (1 B200): HMC, 4 chains SU(3) DIM=4 32x32x32x32, 50 MD steps/trajectory"
+    if config == "batch64":
+        return "link-updates/s (1 B200): HMC, 64 uneven chains NC 2-8, DIM 2-4, 20 MD steps/trajectory"
+    cfg = CONFIGS[config]
+    return (f"link-updates/s (1 B200): HMC, SU({cfg['nc']}) DIM={len(cfg['dims'])} "
+            f"{'x'.join(map(str, cfg['dims']))}, {cfg['nsteps']} MD steps/trajectory")
+
+
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 FALLBACK_BF16_TFLOPS = 1590.0
@@ -76,12 +91,14 @@ def tf32_peak():
 
 
 def fp32_peak(device):
-    """Measured FP32 FFMA peak of the device, TFLOP/s (askja_peak_flops)."""
+    """Measured FP32 FFMA peak of the device, TFLOP/s (askja_peak_flops of the
+    bench-only helper library askja_b200/libaskja_peak.so)."""
     import ctypes
 
-    import askja_b200 as ab
+    lib = ctypes.CDLL(os.path.join(ROOT, "askja_b200", "libaskja_peak.so"))
+    lib.askja_peak_flops.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
     g = ctypes.c_double()
-    rc = ab.library().askja_peak_flops(int(device), 0, 5, ctypes.byref(g))
+    rc = lib.askja_peak_flops(int(device), 0, 5, ctypes.byref(g))
     return g.value / 1e3 if rc == 0 else float("nan")
 
 
@@ -247,6 +264,18 @@ def time_fused_kernel(e, stream_ptr, device, nlaunch, dt):
     return (t1.elapsed_time(t2) - t0.elapsed_time(t1)) / nlaunch
 
 
+def thermalised_links(cfg, ntraj, seed, dev):
+    """Haar hot start, then `ntraj` untimed FP32-mixed trajectories (CUDA graph);
+    returns the links in U-conf layout (FP64)."""
+    import askja_b200 as ab
+    with ab.Engine(cfg["nc"], cfg["dims"], beta=cfg["beta"], dt=cfg["dt"], level=cfg["level"], precision="fp32",
+                   device=dev, seed=seed + 3) as e:
+        e.hot_start(seed + 1)
+        if ntraj:
+            e.run_trajectories(ntraj, cfg["nsteps"], use_graph=True, want_log=False)
+        return e.get_links()
+
+
 def run_ours(args):
     import torch
 
@@ -261,10 +290,13 @@ def run_ours(args):
     torch.cuda.set_device(dev)
     seed = 20240601 + 7919 * rank
     res = {}
+    # untimed: Haar hot start, then FP32-mixed trajectories until the chain has left the
+    # hot-start transient, so that both timed legs start from the same equilibrated links
+    u0 = thermalised_links(cfg, args.therm, seed, dev)
     for prec in ("fp32", "fp64"):
         with ab.Engine(nc, dims, beta=cfg["beta"], dt=cfg["dt"], level=cfg["level"], precision=prec, device=dev,
                        seed=seed) as e:
-            e.hot_start(seed + 1)
+            e.set_links(u0)
             e.initializeE(seed, 0)
             # untimed: picks the kernel mapping for this (NC, DIM, precision); --no-tune keeps the
             # default mapping (under a profiler the candidates' timings are not representative)
@@ -343,7 +375,7 @@ def run_ours(args):
                              / (f32["kernel_ms"] / 1e3) / 1e12 / pk32}}
     field_mb = links * nc * nc * 8 / 1e6
     line = {
-        "metric": f"link-updates/s (1 B200): FP32-mixed HMC trajectories, SU({nc}) {'x'.join(map(str, dims))}",
+        "metric": metric_for(args.config),
         "value": f32["lu"],
         "unit": "link-updates/s",
         "n_gpus": world,
@@ -354,10 +386,12 @@ def run_ours(args):
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "fp32 (links, complex) / fp64 (dH, Metropolis)",
-        "data": "synthetic: seeded Haar hot start, Philox momenta",
+        "data": f"synthetic: seeded Haar hot start, {args.therm} untimed FP32 thermalisation trajectories, "
+                "Philox momenta",
         "config": {"workload": f"{args.config}: SU({nc}) DIM={len(dims)} {'x'.join(map(str, dims))}, "
                                f"BETA={cfg['beta']}, DT={cfg['dt']}, LEVEL={cfg['level']}, "
                                f"{nsteps} MD steps/trajectory, 1 step = 1 trajectory",
+                   "thermalisation_trajectories": args.therm,
                    "links": links, "md_steps_per_traj": nsteps, "parallelism": f"replicas x{world}",
                    "l2": f"links {field_mb:.0f} MB FP32 / {2 * field_mb:.0f} MB FP64 per field; "
                          f"{'inputs larger than L2' if 2 * field_mb > 126 else 'fields partly L2-resident'}"},
@@ -377,6 +411,14 @@ def run_ours(args):
         "gpu_launches": f32["K"] * (nsteps + 15) + f64["K"] * (nsteps + 15),
         "clocks": f32["clocks"],
     }
+    if args.config == "su3_32" and not args.no_batch:
+        # the north-star path: FP32-mixed chains batched in one engine vs each chain alone in FP64
+        b = run_batch(argparse.Namespace(config="batch_su3_32", steps=max(3, args.steps // 2), warmup=args.warmup,
+                                         therm=args.batch_therm))
+        line["batched"] = {k: b[k] for k in ("metric", "value", "unit", "steps", "ms_per_step", "alone_fp64",
+                                             "alone_fp32", "batched_over_alone_fp64", "batched_over_alone_fp32",
+                                             "acceptance_mean", "acceptance_min", "clocks")}
+        line["batched"]["workload"] = b["config"]["workload"]
     if not args.no_precision:
         line["precision"] = precision_report(cfg, dev)
     if not args.no_cpu_baseline:
@@ -505,6 +547,22 @@ def run_reference_sample(cfg, steps, warmup):
             "seconds_per_md_step": per, "times": times}
 
 
+def run_reference_chains(chains, steps, warmup):
+    """The reference CPU code over every chain of a batch in turn (one MD step
+    of each per bench step): aggregate link-updates/s."""
+    tot_links, tot_s, parts = 0, 0.0, []
+    for c in chains:
+        cfg = dict(nc=c["nc"], dims=c["dims"], beta=c["beta"], dt=c["dt"], level=c["level"])
+        r = run_reference_sample(cfg, steps, warmup)
+        links = int(np.prod(c["dims"])) * len(c["dims"])
+        tot_links += links
+        tot_s += r["seconds_per_md_step"]
+        parts.append(r)
+    return {"value": tot_links / tot_s, "unit": "link-updates/s", "cores": parts[0]["cores"], "kind": parts[0]["kind"],
+            "sample": f"{steps} MD step(s) of each of the {len(chains)} chains in turn, OMP threads={parts[0]['cores']}",
+            "seconds_per_md_step": tot_s}
+
+
 def batch_chains(n=64, seed=7):
     """64 uneven chains: NC cycling over {2,3,4,8}, DIM over {2,3,4}, extents
     16^2 .. 16^4 (incl. 4x16^3), BETA uniform over [2,4] * NC^2/3."""
@@ -559,8 +617,11 @@ def run_batch(args):
     nsteps = 50 if su3 else 20
     chains = batch_su3_32_chains() if su3 else tune_dt(batch_chains(), nsteps, dev=dev)
     work = sum(int(np.prod(c["dims"])) * len(c["dims"]) for c in chains) * nsteps
+    therm = getattr(args, "therm", 0)
     with ab.Batch(chains, precision="fp32", device=dev) as b:
         b.hot_start(5)
+        b.run(therm, nsteps)  # untimed thermalisation
+        start = [b.get_links(c) for c in range(len(chains))]
         b.run(args.warmup, nsteps)
         s, t0, t1 = event_timer(b.stream_ptr, dev)
         torch.cuda.synchronize()
@@ -577,10 +638,10 @@ def run_batch(args):
     alone = {}
     for prec in ("fp64", "fp32"):
         tot_ms = 0.0
-        for c in chains:
+        for ci, c in enumerate(chains):
             with ab.Engine(c["nc"], c["dims"], beta=c["beta"], dt=c["dt"], level=c["level"], precision=prec,
                            device=dev, seed=c["seed"]) as e:
-                e.hot_start(5)
+                e.set_links(start[ci])
                 e.run_trajectories(2, nsteps, use_graph=True, want_log=False)
                 s, a, z = event_timer(e.stream_ptr, dev)
                 e.sync()
@@ -590,15 +651,16 @@ def run_batch(args):
                 z.synchronize()
                 tot_ms += a.elapsed_time(z)
         alone[prec] = work * args.steps / (tot_ms / 1e3)
+    metric = metric_for(args.config)
     if su3:
-        metric = "link-updates/s (1 B200): 4 SU(3) 32^4 chains, FP32-mixed batched vs each chain alone in FP64"
         workload = (f"batch_su3_32: 4 chains SU(3) DIM=4 32^4, BETA 5.85/5.95/6.05/6.15, DT=0.02, LEVEL=6, "
-                    f"{nsteps} MD steps/trajectory, 1 step = 1 trajectory of every chain")
+                    f"{nsteps} MD steps/trajectory, {therm} untimed thermalisation trajectories, "
+                    "1 step = 1 trajectory of every chain, FP32-mixed batched vs each chain alone in FP64")
     else:
-        metric = "link-updates/s (1 B200): 64 uneven chains, FP32-mixed batched vs each chain alone in FP64"
         workload = ("batch64: NC in {2,3,4,8}, DIM in {2,3,4}, 16^2..16^4 incl. 4x16^3, "
                     f"BETA in [2,4]*NC^2/3, {nsteps} MD steps/trajectory, DT tuned per chain, "
-                    "1 step = 1 trajectory of every chain")
+                    f"{therm} untimed thermalisation trajectories, "
+                    "1 step = 1 trajectory of every chain, FP32-mixed batched vs each chain alone in FP64")
     return {
         "metric": metric,
         "value": batched, "unit": "link-updates/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
@@ -618,17 +680,22 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return None
-    cfg = CONFIGS[args.config]
-    r = run_reference_sample(cfg, args.steps, args.warmup)
-    nc, dims = cfg["nc"], cfg["dims"]
+    if args.config == "batch64":
+        r = run_reference_chains(batch_chains(), args.steps, args.warmup)
+        workload = "batch64: each of the 64 chains in turn"
+    else:
+        cfg = CONFIGS["su3_32" if args.config == "batch_su3_32" else args.config]
+        r = run_reference_sample(cfg, args.steps, args.warmup)
+        nc, dims = cfg["nc"], cfg.get("cpu_dims", cfg["dims"])
+        workload = f"{args.config}: SU({nc}) DIM={len(dims)} {'x'.join(map(str, dims))}"
     line = {
         "impl": "reference",
-        "metric": "link-updates/s (1 B200): FP32-mixed HMC trajectories, SU(3) 32^4",
+        "metric": metric_for(args.config),
         "value": r["value"], "unit": "link-updates/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": r["seconds_per_md_step"] * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "fp64", "data": "synthetic: seeded Haar links",
-        "config": {"workload": f"{args.config}: SU({nc}) DIM={len(dims)} {'x'.join(map(str, dims))}; "
-                               "1 step = 1 MD step of the reference CPU code", "parallelism": "CPU OpenMP"},
+        "config": {"workload": f"{workload}; 1 step = 1 MD step of the reference CPU code",
+                   "parallelism": "CPU OpenMP"},
         "cpu_baseline": {k: r[k] for k in ("value", "unit", "cores", "kind", "sample")},
         "e2e": {"value": r["value"], "unit": "link-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -668,8 +735,11 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="su3_32", choices=sorted(CONFIGS) + ["batch64", "batch_su3_32"])
+    ap.add_argument("--config", default="su3_32", choices=sorted(CONFIGS) + list(BATCH_CONFIGS))
     ap.add_argument("--cpu-md-steps", type=int, default=2)
+    ap.add_argument("--therm", type=int, default=100, help="untimed FP32 thermalisation trajectories before timing")
+    ap.add_argument("--batch-therm", type=int, default=50, help="untimed thermalisation of the batched sub-run")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched sub-run of the default line")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-precision", action="store_true")
     ap.add_argument("--kernel-only", action="store_true", help="fused-kernel microbenchmark (profiling)")
@@ -682,7 +752,8 @@ def main():
         line = run_kernel_only(args)
     elif args.impl == "reference":
         line = run_reference(args)
-    elif args.config in ("batch64", "batch_su3_32"):
+    elif args.config in BATCH_CONFIGS:
+        args.therm = args.batch_therm
         line = run_batch(args)
     else:
         line = run_ours(args)

@@ -46,7 +46,13 @@ extern "C" {
 #define ASKJA_ERR_PARSE (-6)       /* malformed params file */
 
 #define ASKJA_FP64 0 /* links, momenta and arithmetic in FP64 (the reference's precision) */
-#define ASKJA_FP32 1 /* FP32 links/momenta/arithmetic, reunitarised; FP64 reductions and dH */
+#define ASKJA_FP32 1 /* FP32-mixed: FP32 arithmetic, FP64 reductions and dH.  NC <= 4 (automatic
+                        kernel path): links and momenta carry bfloat16 residual planes, the
+                        kick and link update accumulate into them exactly, links are projected
+                        onto SU(NC) in FP64 before every trajectory (residual-plane mode).
+                        NC > 4 or kernel paths 1/3: FP32 fields, reunitarised per update. */
+#define ASKJA_FP32_LEAN 2 /* FP32 fields without residual planes for every NC, reunitarised per
+                             update (the FP32 storage of ASKJA_FP32 for NC > 4) */
 
 #define ASKJA_MAX_DIM 16
 #define ASKJA_MAX_NC 64
@@ -62,7 +68,7 @@ typedef struct {
   double beta;         /* BETA */
   double dt;           /* DT (used by askja_trajectory) */
   int level;           /* LEVEL: Taylor order of exp(i dt P); outside 0..8 acts as 8 (sunmat.h:215-246) */
-  int precision;       /* ASKJA_FP64 or ASKJA_FP32 */
+  int precision;       /* ASKJA_FP64, ASKJA_FP32 or ASKJA_FP32_LEAN */
   int reunitarise;     /* -1 default (on for FP32, off for FP64), 0 off, 1 on.  On: every
                           link update is projected back onto SU(NC); the FP32 row kernels
                           (NC > 4) and tensor cores project onto U(NC) per update and
@@ -120,8 +126,10 @@ ASKJA_API int askja_get_links(askja_ctx* ctx, double* conf);          /* current
 ASKJA_API int askja_get_saved_links(askja_ctx* ctx, double* conf);    /* uconf (what storeconf writes, sun.cpp:289-302) */
 /* which = 0: pi (current momenta), 1: Pi (updated momenta).  Momenta are
  * Hermitian (P_ij = conj(P_ji), real diagonal) as the reference's are; the
- * ASKJA_FP32 SU(3) link update relies on it (P^2, tr P and det P are formed
- * from the real diagonal and the upper triangle). */
+ * FP32 SU(3) link update relies on it (P^2, tr P and det P are formed from
+ * the real diagonal and the upper triangle).  The residual-plane mode stores
+ * momenta as coordinates of Hermitian traceless matrices: an uploaded matrix
+ * is replaced by its Hermitian traceless part. */
 ASKJA_API int askja_set_momenta(askja_ctx* ctx, int which, const double* conf);
 ASKJA_API int askja_get_momenta(askja_ctx* ctx, int which, double* conf);
 ASKJA_API int askja_initializeU(askja_ctx* ctx);                       /* cold start, sun.cpp:194-207; also uconf */
@@ -285,7 +293,12 @@ ASKJA_API int askja_batch_plaquette(askja_batch* b, double* out);
  *    static device array that every GPU loading the library keeps until exit.
  *    Volumes above 2,097,152 sites are rejected with ASKJA_ERR_ARG.
  *  - The first call on a device looks up that array's device address
- *    (cudaGetSymbolAddress); make that first call before any stream capture.
+ *    (cudaGetSymbolAddress) and keeps it for the life of the process; make
+ *    that first call before any stream capture.  Resetting the device
+ *    (cudaDeviceReset) while the library is loaded is not supported: the kept
+ *    address would no longer be valid.
+ *  - p->device is made current for the call and the caller's own current
+ *    device is restored before returning.
  *  - Work is enqueued on `stream` (NULL: the default stream) and the call
  *    returns without waiting; `out` is valid once the stream reaches it.
  *  - All calls share the one array (it keeps the last call's partials, each
@@ -293,12 +306,6 @@ ASKJA_API int askja_batch_plaquette(askja_batch* b, double* out);
  *    that overlap on the GPU race: serialise them on one stream.
  *  - Errors are reported through askja_last_error(NULL). */
 ASKJA_API int askja_plaqexp_static(const askja_params* p, const void* links, double* out, void* stream);
-
-/* ---- diagnostics (not in the reference) -------------------------------- */
-/* Measured compute-pipe peak of `device` for the roofline: which = 0 FP32
- * FFMA, 1 FP32 packed FFMA2, 2 FP64 DFMA; GFLOP/s (2 flops per FMA lane),
- * best of `repeats` launches.  Allocates a small scratch buffer. */
-ASKJA_API int askja_peak_flops(int device, int which, int repeats, double* gflops);
 
 /* ---- host I/O (no GPU needed) ----------------------------------------- */
 /* Contents of the positional params file (sun.cpp:803-938).  Key names are

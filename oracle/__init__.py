@@ -26,7 +26,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 BUILD = os.path.join(HERE, "_build")
 REF_DIR = os.path.join(HERE, "_ref")
 ORACLE_SO = os.path.join(BUILD, "libaskja_oracle.so")
-REFERENCE_ROOT = "/root/reference"
+# where the reference sources are read from when oracle/_ref is built (absent: not built)
+REFERENCE_ROOT = os.environ.get("ASKJA_REFERENCE", "/root/reference")
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)

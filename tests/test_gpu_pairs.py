@@ -99,13 +99,13 @@ def test_trajectories_match_thread_per_link():
     dims = [4, 4, 4, 6]
     O, u, pi, beta = setup(dims, 3)
     logs = {}
-    for path, prec in [(3, "fp32"), (0, "fp32"), (0, "fp64")]:
+    for path, prec in [(3, "fp32"), (0, "fp32-lean"), (0, "fp64")]:
         with ab.Engine(3, dims, beta=beta, dt=0.02, level=6, precision=prec, kernel_path=path, seed=11) as e:
             e.set_links(u)
             last, log = e.run_trajectories(4, 25, use_graph=True)
             assert last["n_tot"] == 4
             logs[(path, prec)] = log
-    a, b, c = logs[(3, "fp32")], logs[(0, "fp32")], logs[(0, "fp64")]
+    a, b, c = logs[(3, "fp32")], logs[(0, "fp32-lean")], logs[(0, "fp64")]
     assert np.all(np.isfinite(a))
     np.testing.assert_allclose(a[:, 0], b[:, 0], rtol=1e-5)
     assert np.abs(a[:, 2] - b[:, 2]).max() < 2e-3
@@ -121,12 +121,15 @@ def test_path_validation():
         ab.Engine(2, [4, 4], beta=1.0, precision="fp32", kernel_path=3)
     with pytest.raises(ab.AskjaError):
         ab.Engine(3, [4], beta=1.0, precision="fp32", kernel_path=3)
-    with ab.Engine(3, [4, 3], beta=1.0, precision="fp32") as e:
+    with ab.Engine(3, [4, 3], beta=1.0, precision="fp32-lean") as e:
         with pytest.raises(ab.AskjaError):
             ab.set_tuning(e, {"path": 3})
-    with ab.Engine(3, [3, 4], beta=1.0, precision="fp32") as e:
+    with ab.Engine(3, [3, 4], beta=1.0, precision="fp32-lean") as e:
         ab.set_tuning(e, {"path": 3})
         ab.set_tuning(e, {"path": 0})
+    with ab.Engine(3, [3, 4], beta=1.0, precision="fp32") as e:
+        with pytest.raises(ab.AskjaError):  # the residual-plane mode has the thread-per-link mapping only
+            ab.set_tuning(e, {"path": 3})
 
 
 def test_pair_tuning_applied_explicitly():
@@ -136,7 +139,7 @@ def test_pair_tuning_applied_explicitly():
     run on it."""
     dims = [4, 4, 4, 4]
     O, u, pi, beta = setup(dims, 8)
-    with ab.Engine(3, dims, beta=beta, precision="fp32") as e:
+    with ab.Engine(3, dims, beta=beta, precision="fp32-lean") as e:
         e.set_links(u)
         t = ab.autotune(e, reps=2)
         assert 3 not in [c["path"] for c in t["candidates"]]

@@ -42,13 +42,26 @@ def test_restatement_matches_reference(nc, dims):
     np.testing.assert_allclose(fourier(u, O, nc), R.FourierTrafo(), rtol=1e-12, atol=1e-13)
 
 
+def _traceless_hermitian(p):
+    m = p.reshape(-1, p.shape[-1], p.shape[-1])
+    h = 0.5 * (m + np.conj(np.swapaxes(m, 1, 2)))
+    h -= np.trace(h, axis1=1, axis2=2)[:, None, None] / m.shape[-1] * np.eye(m.shape[-1])
+    return h.reshape(p.shape)
+
+
 @pytest.mark.gpu
-@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("precision", ["fp64", "fp32-lean", "fp32"])
 @pytest.mark.parametrize("nc,dims", CASES + [(16, [2, 2, 3]), (40, [3, 2])], ids=IDS + ["su16_2x2x3", "su40_3x2"])
 def test_gpu_tab_and_fourier(nc, dims, precision):
     O, u, pi, Pi = setup(nc, dims, nc * 11 + len(dims))
-    if precision == "fp32":  # compare on the FP32-rounded fields the engine holds
+    tol = 1e-11
+    if precision != "fp64":  # compare on the FP32-rounded fields the engine holds
         u, pi, Pi = (x.astype(np.complex64).astype(np.complex128) for x in (u, pi, Pi))
+        if precision == "fp32" and nc <= 4:
+            # residual-plane mode: momenta are held as Hermitian traceless
+            # coordinates and Tab reads FP32 matrices made from them
+            pi, Pi = _traceless_hermitian(pi), _traceless_hermitian(Pi)
+            tol = 2e-6
     npt = min(O.dim + 2, 6)
     with ab.Engine(nc, dims, beta=2.0 * nc, precision=precision) as e:
         e.set_links(u)
@@ -58,10 +71,10 @@ def test_gpu_tab_and_fourier(nc, dims, precision):
         one = e.Tab(O.vol - 1, npt, mdata=np.ones(npt))
         coef = e.FourierTrafo()
     for i in range(O.vol):
-        np.testing.assert_allclose(allv[i], tab_site(u, pi, Pi, O, i, npt), rtol=1e-11, atol=1e-11)
+        np.testing.assert_allclose(allv[i], tab_site(u, pi, Pi, O, i, npt), rtol=tol, atol=tol)
     np.testing.assert_allclose(one, 1.0 + allv[O.vol - 1], rtol=1e-14)
     np.testing.assert_allclose(coef, fourier(u, O, nc), rtol=1e-11, atol=1e-12)
-    if Reference.available() and nc <= 5:
+    if Reference.available() and nc <= 5 and tol < 1e-10:
         R = Reference(nc, dims, beta=2.0 * nc)
         R.set("u", u)
         R.set("pi", pi)
