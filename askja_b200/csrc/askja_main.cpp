@@ -10,7 +10,8 @@
 //    (RANDOM=0: 120351616, RANDOM=1 and every resume: time(NULL)), not GSL;
 //  - the Wilson- file's eigenphase columns (never initialised by the
 //    reference, sun.cpp:1119) are written as 0;
-//  - `--fp32` selects the FP32 engine (default FP64, the reference's precision).
+//  - `--fp32` selects the FP32 engine (default FP64, the reference's precision);
+//    it projects every accepted configuration onto SU(NC) before saving it.
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -224,6 +225,10 @@ int main(int argc, char** argv) {
           rp.nrec++;
         }
       }
+      // FP32: an accepted configuration is projected onto SU(NC) (in FP64 in the
+      // residual-plane mode, whose link updates are not projected) before it is
+      // saved, so every trajectory starts from projected links
+      if (accept && precision == ASKJA_FP32 && askja_reunitarise(ctx)) return die(ctx, "reunitarise");
       if (accept ? askja_takeconfiguration(ctx) : askja_loadconfiguration(ctx)) return die(ctx, "configuration");
       if (askja_initializeE(ctx, seed, refresh_counter++)) return die(ctx, "initializeE");
       if (energy(0, &crit)) return die(ctx, "energy");

@@ -22,12 +22,23 @@
 #include <tuple>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/askja_gpu.h"
 #include "launch.h"
 #include "misc.cuh"
 #include "split.h"
 
 using askja::DevGuard;
+
+// NVTX range over one host call or enqueue phase (visible to Nsight tools;
+// free when no tool is attached)
+struct Range {
+  explicit Range(const char* name) { nvtxRangePushA(name); }
+  ~Range() { nvtxRangePop(); }
+  Range(const Range&) = delete;
+  Range& operator=(const Range&) = delete;
+};
 using askja::KernelSet;
 using askja::Lat;
 using askja::LaunchCtx;
@@ -262,6 +273,7 @@ int fused_steps(askja_ctx* c, int n, double first_kick, double dt) {
 
 // Enqueue one whole trajectory (no host synchronisation; graph-capturable).
 int enqueue_trajectory(askja_ctx* c, int nsteps) {
+  Range r("askja: enqueue trajectory");
   const double dt = c->p.dt;
   if (c->split && c->lc.reunit) {
     // residual-plane mode: the link updates are not projected; every
@@ -282,12 +294,19 @@ int enqueue_trajectory(askja_ctx* c, int nsteps) {
     KL(c->ks->reunit(lc, cur_u(c)), "reunitarise");
     KL(cudaMemcpyAsync(c->Uconf, cur_u(c), c->field_bytes, cudaMemcpyDeviceToDevice, c->stream), "save links");
   }
-  KL(refresh_launch(c, c->p.seed, &c->st->traj, 0), "refresh");
-  KL(plaq_launch(c), "plaq");
-  KL(linksums_launch(c, 0, -1, false), "kinetic");
-  askja::misc::k_energy<<<1, 1, 0, c->stream>>>(c->sums, c->p.beta, c->N, &c->st->h_old);
-  KL(cudaGetLastError(), "energy");
-  if (int rc = fused_steps(c, nsteps, 0.5 * dt, dt)) return rc;
+  {
+    Range rh("askja: refresh + H_old");
+    KL(refresh_launch(c, c->p.seed, &c->st->traj, 0), "refresh");
+    KL(plaq_launch(c), "plaq");
+    KL(linksums_launch(c, 0, -1, false), "kinetic");
+    askja::misc::k_energy<<<1, 1, 0, c->stream>>>(c->sums, c->p.beta, c->N, &c->st->h_old);
+    KL(cudaGetLastError(), "energy");
+  }
+  {
+    Range rl("askja: leapfrog");
+    if (int rc = fused_steps(c, nsteps, 0.5 * dt, dt)) return rc;
+  }
+  Range rm("askja: H_new + Metropolis");
   KL(force_launch(c, 0, 0, 0, 0.5 * dt, 0.0), "kick");
   KL(plaq_launch(c), "plaq");
   KL(linksums_launch(c, 0, -1, false), "kinetic");
@@ -577,6 +596,7 @@ int askja_create(const askja_params* p, askja_ctx** out) {
 
 int askja_set_links(askja_ctx* c, const double* conf) {
   if (int rc = check_ctx(c)) return rc;
+  Range range("askja_set_links");
   if (!conf) return set_err(c, ASKJA_ERR_ARG, "null buffer");
   DevGuard g(c->p.device);
   if (int rc = upload_conf(c, conf, cur_u(c))) return rc;
@@ -620,6 +640,7 @@ int askja_set_links_async(askja_ctx* c, const double* conf) {
 
 int askja_get_links(askja_ctx* c, double* conf) {
   if (int rc = check_ctx(c)) return rc;
+  Range range("askja_get_links");
   if (!conf) return set_err(c, ASKJA_ERR_ARG, "null buffer");
   DevGuard g(c->p.device);
   return download_conf(c, cur_u(c), conf);
@@ -950,6 +971,7 @@ int askja_Tab_all(askja_ctx* c, int npt, double* out) {
 
 int askja_leapfrog(askja_ctx* c, int nsteps, double eps) {
   if (int rc = check_ctx(c)) return rc;
+  Range range("askja_leapfrog");
   if (nsteps < 1) return set_err(c, ASKJA_ERR_ARG, "nsteps must be >= 1");
   DevGuard g(c->p.device);
   if (int rc = fused_steps(c, nsteps, 0.5 * eps, eps)) return rc;
@@ -960,6 +982,7 @@ int askja_leapfrog(askja_ctx* c, int nsteps, double eps) {
 
 int askja_md_steps(askja_ctx* c, int nsteps, double eps) {
   if (int rc = check_ctx(c)) return rc;
+  Range range("askja_md_steps");
   if (nsteps < 0) return set_err(c, ASKJA_ERR_ARG, "nsteps must be >= 0");
   if (nsteps == 0) return ASKJA_OK;
   DevGuard g(c->p.device);
@@ -976,6 +999,7 @@ int askja_md_steps(askja_ctx* c, int nsteps, double eps) {
 
 int askja_trajectory(askja_ctx* c, int nsteps, askja_traj_result* out) {
   if (int rc = check_ctx(c)) return rc;
+  Range range("askja_trajectory");
   if (nsteps < 1) return set_err(c, ASKJA_ERR_ARG, "nsteps must be >= 1");
   DevGuard g(c->p.device);
   if (int rc = enqueue_trajectory(c, nsteps)) return rc;
@@ -1028,6 +1052,7 @@ int askja_trajectory_async(askja_ctx* c, int nsteps, askja_traj_result* out) {
 int askja_run_trajectories(askja_ctx* c, int ntraj, int nsteps, int use_graph, askja_traj_result* last,
                            double* log) {
   if (int rc = check_ctx(c)) return rc;
+  Range range("askja_run_trajectories");
   if (nsteps < 1 || ntraj < 0) return set_err(c, ASKJA_ERR_ARG, "bad trajectory counts");
   DevGuard g(c->p.device);
   TrajState st0;
@@ -1065,6 +1090,7 @@ int askja_set_tuning(askja_ctx* c, const askja_tuning* t) {
 
 int askja_autotune(askja_ctx* c, int reps, askja_tuning* out) {
   if (int rc = check_ctx(c)) return rc;
+  Range range("askja_autotune");
   if (reps < 1) reps = 5;
   DevGuard g(c->p.device);
   struct Cand {
@@ -1156,6 +1182,15 @@ int askja_autotune(askja_ctx* c, int reps, askja_tuning* out) {
     g_tune_cache[std::make_tuple(c->N, c->D, c->p.precision)] = res;
   }
   if (out) *out = res;
+  return ASKJA_OK;
+}
+
+int askja_tc_wait_selftest(askja_ctx* c, long long cycles) {
+  if (int rc = check_ctx(c)) return rc;
+  if (c->lc.force_rows != 2) return set_err(c, ASKJA_ERR_ARG, "the bounded-wait self-test needs the tensor-core path");
+  if (cycles < 0) return set_err(c, ASKJA_ERR_ARG, "cycles must be >= 0");
+  DevGuard g(c->p.device);
+  KL(c->ks->wait_probe(c->lc, cycles), "bounded-wait self-test");
   return ASKJA_OK;
 }
 

@@ -449,9 +449,26 @@ cudaError_t tab_sites(const LaunchCtx& c, const void* U, const void* Pa, const v
 }
 
 template <typename T>
+cudaError_t wait_probe(const LaunchCtx& c, long long cycles) {
+  if constexpr (sizeof(T) == 4) {
+    if (!c.status) return cudaErrorInvalidValue;
+    if (c.lat.N == 32) {
+      tc::k_wait_probe<32><<<1, tc::THREADS, 0, c.stream>>>(c.status, cycles);
+      return cudaGetLastError();
+    }
+    if (c.lat.N == 64) {
+      tc::k_wait_probe<64><<<1, tc::THREADS, 0, c.stream>>>(c.status, cycles);
+      return cudaGetLastError();
+    }
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <typename T>
 constexpr KernelSet make_set() {
   return KernelSet{&force<T>,   &drift<T>,   &reunit<T>,  &plaq<T>,           &linksums<T>,  &gauss<T>, &lines<T>,
-                   &slice_trace<T>, &line_eigs<T>, &refresh<T>, &identity<T>, &gauss_matrices<T>, &from_conf<T>, &to_conf<T>, &pair_swap<T>, &fourier<T>, &tab_sites<T>};
+                   &slice_trace<T>, &line_eigs<T>, &refresh<T>, &identity<T>, &gauss_matrices<T>, &from_conf<T>, &to_conf<T>, &pair_swap<T>, &fourier<T>, &tab_sites<T>,
+                   &wait_probe<T>};
 }
 
 }  // namespace detail

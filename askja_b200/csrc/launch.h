@@ -92,6 +92,8 @@ struct KernelSet {
   // Tab for nsites sites from site0 with momenta Pa + Pb: out[k*npt + m]
   cudaError_t (*tab)(const LaunchCtx&, const void* U, const void* Pa, const void* Pb, int site0, int nsites, int npt,
                      double* out);
+  // tensor-core path: the give-up path of a bounded wait, on one CTA (tc::k_wait_probe)
+  cudaError_t (*wait_probe)(const LaunchCtx&, long long cycles);
 };
 
 // size (in doubles) of the partial buffer the reductions need

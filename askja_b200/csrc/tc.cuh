@@ -93,13 +93,13 @@ __device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// bounded wait: false after ~2^31 clock cycles (about a second); the clock is
-// read once every 64 polls
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// bounded wait: false after `limit` clock cycles (default 2^31, about a
+// second); the clock is read once every 64 polls
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long long limit = 1LL << 31) {
   const long long t0 = clock64();
   for (uint32_t n = 1;; n++) {
     if (mbar_try(bar, parity)) return true;
-    if ((n & 63u) == 0 && clock64() - t0 > (1LL << 31)) return false;
+    if ((n & 63u) == 0 && clock64() - t0 > limit) return false;
   }
 }
 
@@ -735,6 +735,37 @@ __global__ void __launch_bounds__(THREADS, NC == 64 ? 1 : 3)
     // one more bounded wait before the columns are released
     mbar_wait(s.bar, (phase - 1) & 1u);
   }
+  fence_before();
+  __syncthreads();
+  if (tid < 32) {
+    fence_after();
+    tmem_dealloc(tbase, SH::TMEM_COLS);
+  }
+}
+
+// The give-up path of k_link without a tensor-core instruction: one CTA sets
+// up as k_link does (mbarrier, the same TMEM columns), then thread 0 waits
+// with a limit of `cycles` on the mbarrier's first phase, which nothing ever
+// completes (no MMA is issued, nothing commits), records the timeout in
+// *status exactly as k_link does, and the columns are released (nothing is in
+// flight).  Lets a test check that a bounded wait ends, reports, and leaves
+// the context usable.
+template <int NC>
+__global__ void __launch_bounds__(THREADS) k_wait_probe(unsigned* status, long long cycles) {
+  using SH = Shape<NC>;
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t slot;
+  const int tid = threadIdx.x;
+  if (tid == 0) mbar_init(&bar);
+  if (tid < 32) tmem_alloc(&slot, SH::TMEM_COLS);
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const uint32_t tbase = slot;
+  __shared__ int ok;
+  if (tid == 0) ok = mbar_wait(&bar, 0u, cycles) ? 1 : 0;
+  __syncthreads();
+  if (!ok && tid == 0) atomicOr(status, 1u);
   fence_before();
   __syncthreads();
   if (tid < 32) {

@@ -102,6 +102,19 @@ def fp32_peak(device):
     return g.value / 1e3 if rc == 0 else float("nan")
 
 
+def link_update_bytes(nc, residual):
+    """Compulsory HBM bytes of one fused kick+drift link update in FP32 (neighbour
+    links counted as cache hits): read and write the link and its momentum.
+    FP32-only storage: 4 x NC^2 complex floats.  Residual-plane mode: the link
+    as NC^2 (float2 + bfloat16 pair) = 12 NC^2 bytes, the momentum as NC^2 - 1
+    FP32 coordinates plus their bfloat16 residuals in ceil((NC^2 - 1) / 2)
+    words; SU(3): 2 x (108 + 48) = 312 bytes."""
+    if not residual:
+        return 4 * nc * nc * 8
+    ncoef = nc * nc - 1
+    return 2 * (12 * nc * nc + 4 * ncoef + 4 * ((ncoef + 1) // 2))
+
+
 def tensor_products_per_link(dim, level, reunit=True):
     """Complex NC x NC products of one fused kick+drift link update on the
     tensor path: 4(D-1) staple products, U S, LEVEL-1 Horner products, E U
@@ -323,8 +336,8 @@ def run_ours(args):
         return None
     f32, f64 = res["fp32"], res["fp64"]
     hbm, peak_kind = peaks()
-    s = 8  # bytes per complex element, FP32
-    bytes_per_lu = 4 * nc * nc * s
+    residual = nc <= 4 and not cfg.get("tensor")  # the residual-plane FP32 mode
+    bytes_per_lu = link_update_bytes(nc, residual)
     achieved = bytes_per_lu * links / (f32["kernel_ms"] / 1e3) / 1e9
     traffic = measured_traffic(args.config)
     if cfg.get("tensor"):
@@ -352,10 +365,12 @@ def run_ours(args):
                     "hbm_achieved_gbs": achieved}
     else:
         paired = f32["tuning"]["path"] == 3
-        kname = "pair::k_force_pair (site pairs, packed FP32x2)" if paired else f"small::k_force<{nc},float,1>"
+        kname = ("pair::k_force_pair (site pairs, packed FP32x2)" if paired else
+                 f"split::k_force<{nc},1> (FP32 + bfloat16 residual planes)" if residual else
+                 f"small::k_force<{nc},float,1>")
         # the FP32 floor beside the HBM one: complex products per link = 4(D-1) + 1 force
-        # products + X^2 and E U of the Cayley-Hamilton exponential (N <= 3; LEVEL Horner
-        # products otherwise), 8 NC^3 flops each, against the FFMA peak measured now
+        # products + X^2 and (E - 1) U of the Cayley-Hamilton exponential (N <= 3; LEVEL
+        # Horner products otherwise), 8 NC^3 flops each, against the FFMA peak measured now
         order = cfg["level"] if 0 <= cfg["level"] <= 8 else 8
         fpl = 8 * nc ** 3 * (4 * (len(dims) - 1) + 1 + (2 if nc <= 3 else order))
         pk32 = fp32_peak(dev)
@@ -445,13 +460,13 @@ def precision_report(cfg, dev):
 
 
 def measured_traffic(config: str):
-    """DRAM bytes (read + write) per launch of the fused kernel from the
-    committed ncu summary of the same workload, or None."""
+    """DRAM bytes (read + write) per launch of the fused kernel (residual-plane
+    mode) from the committed ncu summary of the same workload, or None."""
     import re
     path = os.path.join(ROOT, "profiles", "fused_kick_drift_su3_32x4.md")
     if config != "su3_32" or not os.path.exists(path):
         return None
-    m = re.search(r"traffic_bytes_per_launch_fp32_su3_32:\s*(\d+)", open(path).read())
+    m = re.search(r"traffic_bytes_per_launch_residual_su3_32:\s*(\d+)", open(path).read())
     return int(m.group(1)) if m else None
 
 

@@ -307,6 +307,16 @@ ASKJA_API int askja_batch_plaquette(askja_batch* b, double* out);
  *  - Errors are reported through askja_last_error(NULL). */
 ASKJA_API int askja_plaqexp_static(const askja_params* p, const void* links, double* out, void* stream);
 
+/* ---- diagnostics (not in the reference) -------------------------------- */
+/* Exercises the tensor-core path's bounded wait (context on the tensor-core
+ * mapping, kernel path 2, only): one CTA sets up as the tensor-core link update
+ * does and waits `cycles` clock cycles on an mbarrier that nothing completes
+ * (no tensor-core instruction is issued), records the timeout as the link
+ * update would and releases its tensor memory.  Returns once enqueued; the
+ * next synchronising call (askja_sync) then reports ASKJA_ERR_CUDA with the
+ * message of a link update that gave up waiting, and the context stays usable. */
+ASKJA_API int askja_tc_wait_selftest(askja_ctx* ctx, long long cycles);
+
 /* ---- host I/O (no GPU needed) ----------------------------------------- */
 /* Contents of the positional params file (sun.cpp:803-938).  Key names are
  * read but not checked; the order is: header, NC, DIM, N0..N{DIM-1}, BETA, DT,

@@ -251,3 +251,36 @@ def test_config1_step_by_step_vs_reference(start):
         assert abs((h1 - h0_ref) - (h1_ref - h0_ref)) < 1e-8
         t, s = e.PlaqExp()
         assert t + s == pytest.approx(R.EnergyMag(), rel=1e-12)
+
+
+@pytest.mark.skipif(not Reference.available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("precision,tol_p,tol_u", [("fp64", 1e-12, 1e-12), ("fp32", 5e-5, 5e-6)])
+def test_config2_full_size_step_vs_reference(precision, tol_p, tol_u):
+    """SU(8) 10^4 (40,000 links), BETA 20, DT 0.01, LEVEL 8 at full size: one
+    updateE and one updateUandcopyDown of the engine against the reference's
+    own sun.cpp routines (shim-built harness) on the same Haar links and
+    momenta, and the action after the step."""
+    nc, dims, beta, dt, level = 8, [10, 10, 10, 10], 20.0, 0.01, 8
+    rng = np.random.default_rng(808)
+    O = Oracle(nc, dims)
+    nl = O.vol * O.dim
+    u = fields.haar(nc, nl, rng).reshape(O.shape)
+    pi = fields.momenta(nc, nl, beta, rng, O)
+    R = Reference(nc, dims, beta=beta, level=level)
+    R.threads(os.cpu_count() or 1)
+    for name in ("u", "U"):
+        R.set(name, u)
+    R.set("pi", pi)
+    R.set("Pi", pi)
+    R.updateE(dt)
+    with ab.Engine(nc, dims, beta=beta, dt=dt, level=level, precision=precision, reunitarise=False) as e:
+        e.set_links(u)
+        e.set_momenta(pi, 0)
+        assert e.EnergyMag() == pytest.approx(O.EnergyMag(u), rel=1e-12 if precision == "fp64" else 1e-6)
+        e.updateE(dt)
+        assert rel(e.get_momenta(1), R.get("Pi")) < tol_p
+        R.updateUandcopyDown(dt)
+        e.updateUandcopyDown(dt)
+        assert rel(e.get_links(), R.get("u")) < tol_u
+        assert rel(e.get_momenta(0), R.get("pi")) < tol_p
+        assert e.EnergyMag() == pytest.approx(R.EnergyMag(), rel=1e-12 if precision == "fp64" else 1e-6)

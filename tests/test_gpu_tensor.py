@@ -155,3 +155,23 @@ def test_trajectories_stay_unitary_with_gated_gram_schmidt():
         assert unitarity(e.get_saved_links()) < 3e-6
         # dH stays small at this step size
         assert np.abs(log[:, 2]).max() < 1.0
+
+
+def test_bounded_wait_gives_up_and_context_survives():
+    """The tensor-core path's bounded wait on an mbarrier that nothing
+    completes (askja_tc_wait_selftest, one CTA, no tensor-core instruction
+    issued): the wait ends after its limit, the next synchronising call
+    reports it, and the context then runs normal trajectories."""
+    nc, dims = 32, [2, 2, 2]
+    with ab.Engine(nc, dims, beta=2.0 * nc * nc, dt=0.005, level=8, precision="fp32", kernel_path=2, seed=3) as e:
+        e.hot_start(5)
+        e.tc_wait_selftest(100_000)
+        with pytest.raises(ab.AskjaError) as ex:
+            e.sync()
+        assert ex.value.code == -2 and "gave up waiting" in str(ex.value)
+        e.sync()  # the error is reported once
+        r = e.trajectory(3)
+        assert np.isfinite(r["dh"])
+    with ab.Engine(nc, dims, beta=2.0 * nc * nc, precision="fp32", kernel_path=1) as e:
+        with pytest.raises(ab.AskjaError):
+            e.tc_wait_selftest(1000)  # only on the tensor-core mapping

@@ -2,6 +2,8 @@
 the committed golden fixtures (made by tests/golden/gen_golden.py from the
 reference's sun.cpp/measurements4d.cpp) and, where oracle/_ref is built, the
 reference harness directly on fresh random inputs."""
+import os
+
 import numpy as np
 import pytest
 
@@ -147,3 +149,20 @@ def test_oracle_matches_reference_random(nc, dims):
     assert rel(O.updateU(u, O.updateE(u, pi, 0.03), 0.05, 7), R.get("u")) < 1e-12
     R.set("u", u)
     assert O.EnergyMag(u) == pytest.approx(R.EnergyMag(), rel=1e-12)
+
+
+def test_ensemble_fixture_consistent():
+    """The reference-run ensemble fixture (tests/golden/gen_ensemble.py): its
+    binned series reproduce the Nrav averages the reference's measure4d wrote
+    (printed to 6 digits), and the run kept every trajectory's configuration."""
+    import json
+    fx = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden",
+                                     "ensemble_su3_4x4x4x4.json")))
+    assert fx["taken"] == fx["params"]["trajectories"]
+    n = fx["taken"] - fx["skip"]
+    for k in ("polyakov", "wilson", "plaq_t", "plaq_s"):
+        b = np.asarray(fx["bins"][k])
+        assert len(b) == n // fx["bin"]
+        if len(b) * fx["bin"] == n:
+            assert b.mean() == pytest.approx(fx["nrav"][k], rel=1e-5)
+        assert fx["nrav"][k + "_err"] > 0
