@@ -42,7 +42,7 @@ EXPORTS = [
     "askja_GaussLaw", "askja_UViol", "askja_WilsonLoop", "askja_PolyakovLoop", "askja_WilsonLoopDir",
     "askja_PlaqExp", "askja_scalarLoopcorr", "askja_eigenphases", "askja_trajectory", "askja_run_trajectories", "askja_leapfrog",
     "askja_md_steps", "askja_params_load", "askja_params_store", "askja_file_stem", "askja_conf_write",
-    "askja_conf_read", "askja_host_alloc", "askja_host_free", "askja_plaqexp_static", "askja_tc_wait_selftest",
+    "askja_conf_read", "askja_host_alloc", "askja_host_free", "askja_plaqexp_static", "askja_tc_wait_selftest", "askja_set_reduction_range",
     "askja_batch_create", "askja_batch_destroy", "askja_batch_last_error", "askja_batch_stream",
     "askja_batch_hot_start", "askja_batch_set_links", "askja_batch_get_links", "askja_batch_run",
     "askja_batch_plaquette", "askja_autotune", "askja_set_tuning", "askja_set_links_async", "askja_trajectory_async",
@@ -140,6 +140,7 @@ def library() -> ctypes.CDLL:
     L.askja_leapfrog.argtypes = [vp, ip, ctypes.c_double]
     L.askja_md_steps.argtypes = [vp, ip, ctypes.c_double]
     L.askja_tc_wait_selftest.argtypes = [vp, ctypes.c_longlong]
+    L.askja_set_reduction_range.argtypes = [vp, ctypes.c_long, ctypes.c_long]
     L.askja_params_load.argtypes = [ctypes.c_char_p, ctypes.POINTER(RunParams)]
     L.askja_params_store.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(RunParams), ip, ip]
     L.askja_file_stem.argtypes = [ctypes.POINTER(RunParams), ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
@@ -215,6 +216,10 @@ class Engine:
 
     def sync(self):
         self._ck(self.lib.askja_sync(self._ctx))
+
+    def set_reduction_range(self, s0: int, s1: int):
+        """askja_set_reduction_range: only sites [s0, s1) enter the sums."""
+        self._ck(self.lib.askja_set_reduction_range(self._ctx, int(s0), int(s1)))
 
     def tc_wait_selftest(self, cycles: int):
         """askja_tc_wait_selftest: enqueue the tensor-core path's bounded wait

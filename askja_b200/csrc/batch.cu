@@ -20,8 +20,9 @@
 
 #include "../../include/askja_gpu.h"
 #include "batch.cuh"
-#include "launch.h"
 #include "kernels.cuh"
+#include "launch.h"
+#include "split.h"
 
 using askja::Lat;
 using askja::batch::ChainDev;
@@ -54,6 +55,7 @@ struct askja_batch {
   int* d_refresh_start = nullptr;
   int* d_copy_start = nullptr;
   int n_plaq = 0, n_link = 0, n_refresh = 0, n_copy = 0;
+  bool any_split = false;  // some chain runs the residual-plane mode
   void* staging = nullptr;
   int cur = 0;
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
@@ -120,6 +122,19 @@ cudaError_t launch_force(askja_batch* b, const askja_batch::Group& g, cudaStream
     int maxd = 1;
     for (int c : g.chains) maxd = std::max(maxd, b->desc[c].lat.D);
     const dim3 blk(32 * std::min(maxd, 4));
+    if constexpr (sizeof(T) == 4) {
+      // residual-plane mode (every FP32 chain with NC <= 4)
+#define SPLIT(NN)                                                                                                \
+  if (g.N == NN) {                                                                                               \
+    if (mode)                                                                                                    \
+      kb_force_split<NN, 1><<<grid, blk, 0, st>>>(b->d_desc, g.d_start, g.d_ids, (int)g.chains.size(), b->cur, ks); \
+    else                                                                                                         \
+      kb_force_split<NN, 0><<<grid, blk, 0, st>>>(b->d_desc, g.d_start, g.d_ids, (int)g.chains.size(), b->cur, ks); \
+    return cudaGetLastError();                                                                                   \
+  }
+      SPLIT(2) SPLIT(3) SPLIT(4)
+#undef SPLIT
+    }
     if constexpr (sizeof(T) == 4) {
       if (g.N == 3) {
         if (mode)
@@ -201,6 +216,8 @@ int enqueue_trajectory(askja_batch* b, int nsteps) {
     BCK(cudaMemcpyAsync(d.Uconf, d.U[b->cur], askja::field_elems(d.lat) * sizeof(askja::cpx<T>), cudaMemcpyDeviceToDevice,
                         b->stream));
   }
+  if (b->any_split)
+    kb_reunit_split<<<b->n_refresh, 128, 0, b->stream>>>(b->d_desc, b->d_refresh_start, b->nchains, b->cur);
   kb_refresh<S2><<<b->n_refresh, 128, 0, b->stream>>>(b->d_desc, b->d_refresh_start, b->nchains);
   BCK(cudaGetLastError());
   if (int rc = energies<T>(b, 0)) return rc;
@@ -336,6 +353,7 @@ int askja_batch_create(const askja_chain_params* chains, int nchains, int precis
     // Newton-Schulz step, with a full pass every FULL_REUNIT_EVERY
     // trajectories, as a single chain does
     d.reunit = precision == ASKJA_FP32 ? (p.nc > 4 ? 2 : 1) : 0;
+    if (precision == ASKJA_FP32 && askja::splitk::supported(p.nc)) d.reunit = 0;  // residual planes: per trajectory
     d.seed = p.seed;
     if (int rc = dalloc(b, &d.st, sizeof(TrajState))) return fail(rc);
     if (cudaMemset(d.st, 0, sizeof(TrajState)) != cudaSuccess) return fail(berr(b, ASKJA_ERR_CUDA, "memset"));
@@ -344,10 +362,23 @@ int askja_batch_create(const askja_chain_params* chains, int nchains, int precis
     d.link_blocks = (int)((V * p.dim + askja::misc::RED_THREADS - 1) / askja::misc::RED_THREADS);
     if (int rc = dalloc(b, &d.partial, (2 * (size_t)d.plaq_blocks + d.link_blocks) * sizeof(double))) return fail(rc);
     d.n16 = (long)(fbytes / 16);
+    if (precision == ASKJA_FP32 && askja::splitk::supported(p.nc)) {
+      // residual-plane mode, as a single FP32 chain of this colour number:
+      // projected onto SU(N) in FP64 before every trajectory, not per update
+      const size_t lo_bytes = askja::field_elems(L) * sizeof(uint32_t);
+      for (void** f : {&d.UL[0], &d.UL[1], &d.ULconf})
+        if (int rc = dalloc(b, f, lo_bytes)) return fail(rc);
+      if (int rc = dalloc(b, &d.PC, askja::splitk::coef_floats(L) * sizeof(float))) return fail(rc);
+      if (int rc = dalloc(b, &d.PCL, askja::splitk::coef_words(L) * sizeof(uint32_t))) return fail(rc);
+      for (void* f : {d.UL[0], d.UL[1], d.ULconf})
+        if (cudaMemset(f, 0, lo_bytes) != cudaSuccess) return fail(berr(b, ASKJA_ERR_CUDA, "memset"));
+      d.n16lo = (long)(lo_bytes / 16);
+      b->any_split = true;
+    }
     plaq_start.push_back(plaq_start.back() + d.plaq_blocks);
     link_start.push_back(link_start.back() + d.link_blocks);
     refresh_start.push_back(refresh_start.back() + (int)((V * p.dim + 127) / 128));
-    copy_start.push_back(copy_start.back() + (int)((d.n16 + 4095) / 4096));
+    copy_start.push_back(copy_start.back() + (int)((d.n16 + 4095) / 4096) + (int)((d.n16lo + 4095) / 4096));
     max_conf = std::max(max_conf, (size_t)V * p.dim * p.nc * p.nc * 16);
     // cold start
     askja::LaunchCtx lc = chain_lc(b, c);
@@ -414,9 +445,15 @@ int askja_batch_hot_start(askja_batch* b, uint64_t seed) {
   for (int c = 0; c < b->nchains; c++) {
     askja::LaunchCtx lc = chain_lc(b, c);
     ChainDev& d = b->desc[c];
-    if (kset(b).gauss_matrices(lc, d.U[b->cur], seed + 1000003ull * c) != cudaSuccess ||
-        kset(b).reunit(lc, d.U[b->cur]) != cudaSuccess)
+    if (kset(b).gauss_matrices(lc, d.U[b->cur], seed + 1000003ull * c) != cudaSuccess)
       return berr(b, ASKJA_ERR_CUDA, "hot start launch");
+    if (d.UL[0]) {
+      BCK(cudaMemsetAsync(d.UL[b->cur], 0, d.n16lo * 16, b->stream));
+      if (askja::splitk::reunit(lc, d.U[b->cur], d.UL[b->cur], d.Uconf, d.ULconf) != cudaSuccess)
+        return berr(b, ASKJA_ERR_CUDA, "hot start launch");
+      continue;
+    }
+    if (kset(b).reunit(lc, d.U[b->cur]) != cudaSuccess) return berr(b, ASKJA_ERR_CUDA, "hot start launch");
     BCK(cudaMemcpyAsync(d.Uconf, d.U[b->cur], d.n16 * 16, cudaMemcpyDeviceToDevice, b->stream));
   }
   BCK(cudaStreamSynchronize(b->stream));
@@ -433,8 +470,11 @@ int askja_batch_set_links(askja_batch* b, int c, const double* conf) {
     if (!std::isfinite(conf[i])) return berr(b, ASKJA_ERR_NONFINITE, "non-finite value in chain %d links", c);
   BCK(cudaMemcpyAsync(b->staging, conf, bytes, cudaMemcpyHostToDevice, b->stream));
   askja::LaunchCtx lc = chain_lc(b, c);
-  if (kset(b).from_conf(lc, b->staging, d.U[b->cur]) != cudaSuccess) return berr(b, ASKJA_ERR_CUDA, "from_conf");
+  const cudaError_t ec = d.UL[0] ? askja::splitk::links_from_conf(lc, b->staging, d.U[b->cur], d.UL[b->cur])
+                                 : kset(b).from_conf(lc, b->staging, d.U[b->cur]);
+  if (ec != cudaSuccess) return berr(b, ASKJA_ERR_CUDA, "from_conf");
   BCK(cudaMemcpyAsync(d.Uconf, d.U[b->cur], d.n16 * 16, cudaMemcpyDeviceToDevice, b->stream));
+  if (d.UL[0]) BCK(cudaMemcpyAsync(d.ULconf, d.UL[b->cur], d.n16lo * 16, cudaMemcpyDeviceToDevice, b->stream));
   BCK(cudaStreamSynchronize(b->stream));
   return ASKJA_OK;
 }
@@ -446,7 +486,9 @@ int askja_batch_get_links(askja_batch* b, int c, double* conf) {
   ChainDev& d = b->desc[c];
   const size_t bytes = (size_t)d.lat.V * d.lat.D * d.lat.N * d.lat.N * 16;
   askja::LaunchCtx lc = chain_lc(b, c);
-  if (kset(b).to_conf(lc, d.U[b->cur], b->staging) != cudaSuccess) return berr(b, ASKJA_ERR_CUDA, "to_conf");
+  const cudaError_t ec = d.UL[0] ? askja::splitk::links_to_conf(lc, d.U[b->cur], d.UL[b->cur], b->staging)
+                                 : kset(b).to_conf(lc, d.U[b->cur], b->staging);
+  if (ec != cudaSuccess) return berr(b, ASKJA_ERR_CUDA, "to_conf");
   BCK(cudaMemcpyAsync(conf, b->staging, bytes, cudaMemcpyDeviceToHost, b->stream));
   BCK(cudaStreamSynchronize(b->stream));
   return ASKJA_OK;

@@ -12,6 +12,7 @@
 #include "misc.cuh"
 #include "rows.cuh"
 #include "small.cuh"
+#include "split.cuh"
 
 namespace askja {
 namespace batch {
@@ -33,6 +34,13 @@ struct ChainDev {
   int plaq_blocks;  // RED_THREADS-site blocks
   int link_blocks;  // RED_THREADS-link blocks
   long n16;         // field size in 16-byte units
+  // residual-plane FP32 mode (FP32 chains with NC <= 4; null otherwise): link
+  // residuals, momentum coordinates and their residuals (split.cuh)
+  void* UL[2];
+  void* ULconf;
+  void* PC;
+  void* PCL;
+  long n16lo;       // residual field size in 16-byte units
 };
 
 // chain owning work item i (item_start has nchains+1 entries, ascending)
@@ -88,6 +96,38 @@ __device__ __forceinline__ void force_small_item(const ChainDev* __restrict__ de
   const int order = sd.order, reunit = sd.reunit;
   for (int mu = threadIdx.x >> 5; mu < L.D; mu += (blockDim.x >> 5))
     small::force_link<N, T, S2, MODE>(L, U, P, P, Uo, ek, ed, order, reunit, mu, x);
+}
+
+// The residual-plane kernel on the same tiles (split::link_update).
+template <int N, int MODE>
+__device__ __forceinline__ void force_split_item(const ChainDev* __restrict__ descs,
+                                                 const int* __restrict__ item_start,
+                                                 const int* __restrict__ chain_ids, int nchains, int cur,
+                                                 double kick_scale) {
+  __shared__ ChainDev sd;
+  const int tile = load_chain(sd, descs, item_start, chain_ids, nchains);
+  const Lat L = sd.lat;
+  const int x = tile * 32 + (threadIdx.x & 31);
+  if (x >= L.V) return;
+  const float2* U = (const float2*)sd.U[cur];
+  const uint32_t* UL = (const uint32_t*)sd.UL[cur];
+  float* P = (float*)sd.PC;
+  uint32_t* PL = (uint32_t*)sd.PCL;
+  float2* Uo = (float2*)sd.U[cur ^ 1];
+  uint32_t* ULo = (uint32_t*)sd.UL[cur ^ 1];
+  const float ek = (float)(kick_scale * sd.dt), ed = (float)sd.dt;
+  const int order = sd.order;
+  for (int mu = threadIdx.x >> 5; mu < L.D; mu += (blockDim.x >> 5))
+    split::link_update<N, MODE>(L, U, UL, P, PL, P, PL, Uo, ULo, ek, ed, order, mu, x);
+}
+
+// SU(3): seven resident CTAs per SM, as the single-chain kernel's tuned budget
+template <int N, int MODE>
+__global__ void __launch_bounds__(128, N == 3 ? 7 : 1) kb_force_split(const ChainDev* __restrict__ descs,
+                                                                       const int* __restrict__ item_start,
+                                                                       const int* __restrict__ chain_ids,
+                                                                       int nchains, int cur, double kick_scale) {
+  force_split_item<N, MODE>(descs, item_start, chain_ids, nchains, cur, kick_scale);
 }
 
 template <int N, typename T, int MODE>
@@ -151,11 +191,21 @@ __global__ void __launch_bounds__(misc::RED_THREADS) kb_plaq(const ChainDev* __r
   const S2* U = (const S2*)sd.U[cur];
   const int s = blk * misc::RED_THREADS + threadIdx.x;
   double v[2] = {0.0, 0.0};
-  switch (sd.lat.N) {
-    case 2: misc::plaq_site<2, S2>(sd.lat, U, s, v); break;
-    case 3: misc::plaq_site<3, S2>(sd.lat, U, s, v); break;
-    case 4: misc::plaq_site<4, S2>(sd.lat, U, s, v); break;
-    default: misc::plaq_site<0, S2>(sd.lat, U, s, v);
+  if (sd.UL[0]) {
+    const float2* Uh = (const float2*)sd.U[cur];
+    const uint32_t* Ul = (const uint32_t*)sd.UL[cur];
+    switch (sd.lat.N) {
+      case 2: split::plaq_site<2>(sd.lat, Uh, Ul, s, v); break;
+      case 3: split::plaq_site<3>(sd.lat, Uh, Ul, s, v); break;
+      default: split::plaq_site<4>(sd.lat, Uh, Ul, s, v);
+    }
+  } else {
+    switch (sd.lat.N) {
+      case 2: misc::plaq_site<2, S2>(sd.lat, U, s, v); break;
+      case 3: misc::plaq_site<3, S2>(sd.lat, U, s, v); break;
+      case 4: misc::plaq_site<4, S2>(sd.lat, U, s, v); break;
+      default: misc::plaq_site<0, S2>(sd.lat, U, s, v);
+    }
   }
   misc::block_sum<2>(v);
   if (threadIdx.x == 0) {
@@ -172,11 +222,21 @@ __global__ void __launch_bounds__(misc::RED_THREADS) kb_kinetic(const ChainDev* 
   const int blk = load_chain(sd, descs, item_start, nullptr, nchains);
   const long t = (long)blk * misc::RED_THREADS + threadIdx.x;
   double v[3] = {0.0, 0.0, 0.0};
-  switch (sd.lat.N) {
-    case 2: misc::link_sums<2, S2>(sd.lat, (const S2*)sd.P, nullptr, nullptr, t, v); break;
-    case 3: misc::link_sums<3, S2>(sd.lat, (const S2*)sd.P, nullptr, nullptr, t, v); break;
-    case 4: misc::link_sums<4, S2>(sd.lat, (const S2*)sd.P, nullptr, nullptr, t, v); break;
-    default: misc::link_sums<0, S2>(sd.lat, (const S2*)sd.P, nullptr, nullptr, t, v);
+  if (sd.PC) {
+    const float* P = (const float*)sd.PC;
+    const uint32_t* PL = (const uint32_t*)sd.PCL;
+    switch (sd.lat.N) {
+      case 2: v[0] = split::kinetic_link<2>(sd.lat, P, PL, t); break;
+      case 3: v[0] = split::kinetic_link<3>(sd.lat, P, PL, t); break;
+      default: v[0] = split::kinetic_link<4>(sd.lat, P, PL, t);
+    }
+  } else {
+    switch (sd.lat.N) {
+      case 2: misc::link_sums<2, S2>(sd.lat, (const S2*)sd.P, nullptr, nullptr, t, v); break;
+      case 3: misc::link_sums<3, S2>(sd.lat, (const S2*)sd.P, nullptr, nullptr, t, v); break;
+      case 4: misc::link_sums<4, S2>(sd.lat, (const S2*)sd.P, nullptr, nullptr, t, v); break;
+      default: misc::link_sums<0, S2>(sd.lat, (const S2*)sd.P, nullptr, nullptr, t, v);
+    }
   }
   misc::block_sum<3>(v);
   // kinetic partials live after the plaquette partials
@@ -217,22 +277,64 @@ __global__ void __launch_bounds__(128) kb_refresh(const ChainDev* __restrict__ d
                                                   int nchains) {
   __shared__ ChainDev sd;
   const int blk = load_chain(sd, descs, item_start, nullptr, nchains);
-  misc::refresh_link<S2>(sd.lat, (S2*)sd.P, sd.seed, (uint32_t)sd.st->traj, sd.scale, (long)blk * 128 + threadIdx.x);
+  const long t = (long)blk * 128 + threadIdx.x;
+  const uint32_t traj = (uint32_t)sd.st->traj;
+  if (sd.PC) {
+    float* P = (float*)sd.PC;
+    uint32_t* PL = (uint32_t*)sd.PCL;
+    switch (sd.lat.N) {
+      case 2: split::refresh_link<2>(sd.lat, P, PL, sd.seed, traj, sd.scale, t); break;
+      case 3: split::refresh_link<3>(sd.lat, P, PL, sd.seed, traj, sd.scale, t); break;
+      default: split::refresh_link<4>(sd.lat, P, PL, sd.seed, traj, sd.scale, t);
+    }
+  } else {
+    misc::refresh_link<S2>(sd.lat, (S2*)sd.P, sd.seed, traj, sd.scale, t);
+  }
 }
 
-// Accept (uconf = u) or reject (u = uconf): item = 4096 x 16 bytes.
+// Residual-plane chains: projection onto SU(N) in FP64 before each
+// trajectory, into the links and the saved copy (split::reunit_link); the
+// other chains' items return at once.  Item = 128-link block (the refresh list).
+static __global__ void __launch_bounds__(128) kb_reunit_split(const ChainDev* __restrict__ descs,
+                                                              const int* __restrict__ item_start, int nchains,
+                                                              int cur) {
+  __shared__ ChainDev sd;
+  const int blk = load_chain(sd, descs, item_start, nullptr, nchains);
+  if (!sd.UL[0]) return;
+  const long t = (long)blk * 128 + threadIdx.x;
+  float2* U = (float2*)sd.U[cur];
+  uint32_t* UL = (uint32_t*)sd.UL[cur];
+  float2* C = (float2*)sd.Uconf;
+  uint32_t* CL = (uint32_t*)sd.ULconf;
+  switch (sd.lat.N) {
+    case 2: split::reunit_link<2>(sd.lat, U, UL, C, CL, t); break;
+    case 3: split::reunit_link<3>(sd.lat, U, UL, C, CL, t); break;
+    default: split::reunit_link<4>(sd.lat, U, UL, C, CL, t);
+  }
+}
+
+// Accept (uconf = u) or reject (u = uconf): item = 4096 x 16 bytes of the
+// links, then (residual-plane chains) of their residuals.
 static __global__ void __launch_bounds__(256) kb_accept_copy(const ChainDev* __restrict__ descs,
                                                              const int* __restrict__ item_start, int nchains,
                                                              int cur) {
   __shared__ ChainDev sd;
   const int blk = load_chain(sd, descs, item_start, nullptr, nchains);
   const bool acc = sd.st->accepted != 0;
+  const long hi_items = (sd.n16 + 4095) / 4096;
+  long i0 = (long)blk * 4096;
   uint4* U = (uint4*)sd.U[cur];
   uint4* C = (uint4*)sd.Uconf;
+  long n = sd.n16;
+  if (blk >= hi_items) {  // residual part
+    i0 = (long)(blk - hi_items) * 4096;
+    U = (uint4*)sd.UL[cur];
+    C = (uint4*)sd.ULconf;
+    n = sd.n16lo;
+  }
   uint4* dst = acc ? C : U;
   const uint4* src = acc ? U : C;
-  const long i0 = (long)blk * 4096;
-  const long i1 = min(sd.n16, i0 + 4096);
+  const long i1 = min(n, i0 + 4096);
   for (long i = i0 + threadIdx.x; i < i1; i += blockDim.x) dst[i] = src[i];
 }
 

@@ -119,7 +119,13 @@ struct Lat {
   const int* nbr;  // nbr[(2*d + 0)*V + s] = s + d^, nbr[(2*d + 1)*V + s] = s - d^
   int n[ASKJA_MAX_DIM];
   int stride[ASKJA_MAX_DIM];
+  // sites [r0, r1) enter the plaquette and link sums (r1 = 0: up to V); a
+  // domain-decomposed chain counts only the sites it owns, not its halo
+  int r0, r1;
 };
+
+// whether site s enters the reductions
+__host__ __device__ __forceinline__ bool counted(const Lat& L, int s) { return s >= L.r0 && (L.r1 == 0 || s < L.r1); }
 
 __device__ __forceinline__ int nb_plus(const Lat& L, int d, int s) { return __ldg(L.nbr + (size_t)(2 * d) * L.V + s); }
 __device__ __forceinline__ int nb_minus(const Lat& L, int d, int s) {

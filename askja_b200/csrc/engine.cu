@@ -279,8 +279,7 @@ int enqueue_trajectory(askja_ctx* c, int nsteps) {
     // residual-plane mode: the link updates are not projected; every
     // trajectory starts from links projected onto SU(N) in FP64 (the saved
     // copy follows, so a rejected trajectory restores projected links)
-    KL(askja::splitk::reunit(c->lc, cur_u(c), cur_ul(c)), "reunitarise");
-    KL(copy_saved(c, true), "save links");
+    KL(askja::splitk::reunit(c->lc, cur_u(c), cur_ul(c), c->Uconf, c->ULconf), "reunitarise");
   } else if (c->lc.reunit && (c->lc.force_rows == 2 || (c->lc.rows_ns && uses_rows(c)))) {
     // the tensor-core link update keeps U' exactly as unitary as U (it
     // projects exp(i eps P), not U'); the rounding defect U accumulates (an
@@ -1182,6 +1181,18 @@ int askja_autotune(askja_ctx* c, int reps, askja_tuning* out) {
     g_tune_cache[std::make_tuple(c->N, c->D, c->p.precision)] = res;
   }
   if (out) *out = res;
+  return ASKJA_OK;
+}
+
+int askja_set_reduction_range(askja_ctx* c, long s0, long s1) {
+  if (int rc = check_ctx(c)) return rc;
+  if (s0 < 0 || s1 <= s0 || s1 > c->V)
+    return set_err(c, ASKJA_ERR_ARG, "reduction range [%ld, %ld) outside [0, %ld)", s0, s1, c->V);
+  c->lat.r0 = (int)s0;
+  c->lat.r1 = (int)s1;
+  c->lc.lat.r0 = c->lat.r0;
+  c->lc.lat.r1 = c->lat.r1;
+  drop_graphs(c);  // the captured launches hold the geometry by value
   return ASKJA_OK;
 }
 

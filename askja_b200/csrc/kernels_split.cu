@@ -72,11 +72,11 @@ cudaError_t drift(const LaunchCtx& c, void* U, void* UL, const void* P, const vo
   });
 }
 
-cudaError_t reunit(const LaunchCtx& c, void* U, void* UL) {
+cudaError_t reunit(const LaunchCtx& c, void* U, void* UL, void* Usave, void* ULsave) {
   return by_nc(c.lat.N, [&](auto n) {
     constexpr int N = decltype(n)::value;
-    split::k_reunit<N><<<blocks_for(nlinks(c.lat), THREADS), THREADS, 0, c.stream>>>(c.lat, (float2*)U,
-                                                                                       (uint32_t*)UL);
+    split::k_reunit<N><<<blocks_for(nlinks(c.lat), THREADS), THREADS, 0, c.stream>>>(
+        c.lat, (float2*)U, (uint32_t*)UL, (float2*)Usave, (uint32_t*)ULsave);
     return cudaGetLastError();
   });
 }

@@ -61,7 +61,7 @@ __global__ void k_finish(const double* __restrict__ partial, int nblocks, double
 template <int NT, typename S2>
 __device__ __forceinline__ void plaq_site(const Lat& L, const S2* __restrict__ U, int s, double (&v)[2]) {
   const int N = NT > 0 ? NT : L.N;
-  if (s < L.V) {
+  if (s < L.V && counted(L, s)) {
     for (int mu = 0; mu < L.D; mu++) {
       const int xpmu = nb_plus(L, mu, s);
       for (int nu = mu + 1; nu < L.D; nu++) {
@@ -105,7 +105,7 @@ template <int NT, typename S2>
 __device__ __forceinline__ void link_sums(const Lat& L, const S2* __restrict__ Pa, const S2* __restrict__ Pb,
                                           const S2* __restrict__ U, long t, double (&v)[3]) {
   const int N = NT > 0 ? NT : L.N;
-  if (t < (long)L.V * L.D) {
+  if (t < (long)L.V * L.D && counted(L, (int)(t % L.V))) {
     const int d = (int)(t / L.V);
     const int s = (int)(t - (long)d * L.V);
     if (Pa) {
@@ -571,8 +571,9 @@ __global__ void __launch_bounds__(RED_THREADS) k_plaq_big(Lat L, const S2* __res
   double v[2] = {trt, trs};
   block_sum<2>(v);
   if (tid == 0) {
-    partial[(size_t)s * 2 + 0] = nt - v[0] / N;
-    partial[(size_t)s * 2 + 1] = ns - v[1] / N;
+    const bool in = counted(L, s);
+    partial[(size_t)s * 2 + 0] = in ? nt - v[0] / N : 0.0;
+    partial[(size_t)s * 2 + 1] = in ? ns - v[1] / N : 0.0;
   }
 }
 
@@ -618,7 +619,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_linksums_big(Lat L, const S2* _
   block_sum<3>(v);
   if (threadIdx.x == 0)
 #pragma unroll
-    for (int k = 0; k < 3; k++) partial[(size_t)t * 3 + k] = v[k];
+    for (int k = 0; k < 3; k++) partial[(size_t)t * 3 + k] = counted(L, s) ? v[k] : 0.0;
 }
 
 // refresh_link with one CTA per link: thread per off-diagonal pair (the pair's

@@ -461,10 +461,11 @@ __global__ void __launch_bounds__(128) k_drift(Lat L, float2* __restrict__ U, ui
 }
 
 // Projection onto SU(N) in FP64 from hi + lo (small::reunitarise: modified
-// Gram-Schmidt of the first N-1 rows, last row completing det = 1).
+// Gram-Schmidt of the first N-1 rows, last row completing det = 1) of link t
+// (t = mu V + x), written back and, when Usave is given, also to (Usave, ULsave).
 template <int N>
-__global__ void __launch_bounds__(128) k_reunit(Lat L, float2* __restrict__ U, uint32_t* __restrict__ UL) {
-  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void reunit_link(const Lat& L, float2* __restrict__ U, uint32_t* __restrict__ UL,
+                                            float2* __restrict__ Usave, uint32_t* __restrict__ ULsave, long t) {
   if (t >= (long)L.V * L.D) return;
   const int mu = (int)(t / L.V);
   const int x = (int)(t - (long)mu * L.V);
@@ -472,16 +473,20 @@ __global__ void __launch_bounds__(128) k_reunit(Lat L, float2* __restrict__ U, u
   load_exact<N>(M, U, UL, L, mu, x);
   small::reunitarise(M);
   store_exact<N>(U, UL, M, L, mu, x);
+  if (Usave) store_exact<N>(Usave, ULsave, M, L, mu, x);
 }
 
-// Plaquette sums (misc::plaq_site) on hi + lo in FP64.
 template <int N>
-__global__ void __launch_bounds__(misc::RED_THREADS) k_plaq(Lat L, const float2* __restrict__ U,
-                                                            const uint32_t* __restrict__ UL,
-                                                            double* __restrict__ partial) {
-  double v[2] = {0.0, 0.0};
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s < L.V) {
+__global__ void __launch_bounds__(128) k_reunit(Lat L, float2* __restrict__ U, uint32_t* __restrict__ UL,
+                                                float2* __restrict__ Usave, uint32_t* __restrict__ ULsave) {
+  reunit_link<N>(L, U, UL, Usave, ULsave, (long)blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// Plaquette sums of site s (misc::plaq_site) on hi + lo in FP64, added to v.
+template <int N>
+__device__ __forceinline__ void plaq_site(const Lat& L, const float2* __restrict__ U, const uint32_t* __restrict__ UL,
+                                          int s, double (&v)[2]) {
+  if (s < L.V && counted(L, s)) {
     for (int mu = 0; mu < L.D; mu++) {
       const int xpmu = nb_plus(L, mu, s);
       small::Mat<N, double> A, B;
@@ -510,11 +515,35 @@ __global__ void __launch_bounds__(misc::RED_THREADS) k_plaq(Lat L, const float2*
       }
     }
   }
+}
+
+template <int N>
+__global__ void __launch_bounds__(misc::RED_THREADS) k_plaq(Lat L, const float2* __restrict__ U,
+                                                            const uint32_t* __restrict__ UL,
+                                                            double* __restrict__ partial) {
+  double v[2] = {0.0, 0.0};
+  plaq_site<N>(L, U, UL, blockIdx.x * blockDim.x + threadIdx.x, v);
   misc::block_sum<2>(v);
   if (threadIdx.x == 0) {
     partial[blockIdx.x * 2 + 0] = v[0];
     partial[blockIdx.x * 2 + 1] = v[1];
   }
+}
+
+// tr(P^2) of link t (t = d V + s) from coordinates hi + lo, 0 past the end
+template <int N>
+__device__ __forceinline__ double kinetic_link(const Lat& L, const float* __restrict__ P,
+                                               const uint32_t* __restrict__ PL, long t) {
+  if (t >= (long)L.V * L.D) return 0.0;
+  const int d = (int)(t / L.V);
+  const int s = (int)(t - (long)d * L.V);
+  if (!counted(L, s)) return 0.0;
+  float h[Dims<N>::NCOEF], l[Dims<N>::NCOEF];
+  double c[Dims<N>::NCOEF];
+  load_coefs<N>(h, l, P, PL, L, d, s);
+#pragma unroll
+  for (int k = 0; k < Dims<N>::NCOEF; k++) c[k] = (double)h[k] + (double)l[k];
+  return coef_tr2<N>(c);
 }
 
 // Per-link sums in FP64 from hi + lo (misc::link_sums):
@@ -530,7 +559,7 @@ __global__ void __launch_bounds__(misc::RED_THREADS) k_linksums(Lat L, const flo
   constexpr int NC = Dims<N>::NCOEF;
   double v[3] = {0.0, 0.0, 0.0};
   const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < (long)L.V * L.D) {
+  if (t < (long)L.V * L.D && counted(L, (int)(t % L.V))) {
     const int d = (int)(t / L.V);
     const int s = (int)(t - (long)d * L.V);
     if (Pa) {
@@ -580,13 +609,10 @@ __global__ void __launch_bounds__(misc::RED_THREADS) k_linksums(Lat L, const flo
 // Momentum refresh into coordinates: the entries misc::refresh_link draws
 // (same Philox stream, FP64), split into hi + lo.
 template <int N>
-__global__ void k_refresh(Lat L, float* __restrict__ P, uint32_t* __restrict__ PL, uint64_t seed,
-                          const unsigned long long* __restrict__ traj_dev, unsigned long long traj_host,
-                          double scale) {
+__device__ __forceinline__ void refresh_link(const Lat& L, float* __restrict__ P, uint32_t* __restrict__ PL,
+                                             uint64_t seed, uint32_t traj, double scale, long t) {
   constexpr int NC = Dims<N>::NCOEF;
-  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long)L.V * L.D) return;
-  const uint32_t traj = (uint32_t)(traj_dev ? *traj_dev : traj_host);
   const int d = (int)(t / L.V);
   const int s = (int)(t - (long)d * L.V);
   double c[NC];
@@ -603,6 +629,14 @@ __global__ void k_refresh(Lat L, float* __restrict__ P, uint32_t* __restrict__ P
 #pragma unroll
   for (int k = 0; k < NC; k++) split_of(c[k], h[k], l[k]);
   store_coefs<N>(P, PL, h, l, L, d, s);
+}
+
+template <int N>
+__global__ void k_refresh(Lat L, float* __restrict__ P, uint32_t* __restrict__ PL, uint64_t seed,
+                          const unsigned long long* __restrict__ traj_dev, unsigned long long traj_host,
+                          double scale) {
+  const uint32_t traj = (uint32_t)(traj_dev ? *traj_dev : traj_host);
+  refresh_link<N>(L, P, PL, seed, traj, scale, (long)blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // ---- conversions to and from the host U-conf layout ([site][dir][row][col][re,im] FP64) ----

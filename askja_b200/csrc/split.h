@@ -26,8 +26,8 @@ cudaError_t force(const LaunchCtx& c, int mode, const void* U, const void* UL, c
                   void* Pout, void* PLout, void* Uout, void* ULout, double ek, double ed);
 // U <- U + (exp(i eps P) - 1) U in place
 cudaError_t drift(const LaunchCtx& c, void* U, void* UL, const void* P, const void* PL, double eps);
-// projection onto SU(N) in FP64
-cudaError_t reunit(const LaunchCtx& c, void* U, void* UL);
+// projection onto SU(N) in FP64, in place and (Usave non-null) also into (Usave, ULsave)
+cudaError_t reunit(const LaunchCtx& c, void* U, void* UL, void* Usave = nullptr, void* ULsave = nullptr);
 // out[0] temporal, out[1] spatial plaquette sums
 cudaError_t plaq(const LaunchCtx& c, const void* U, const void* UL, double* partial, double* out);
 // out[0] sum tr(Pa^2), out[1] sum tr((Pa+Pb)^2)/4, out[2] sum ReTr((UU^dag-1)^2) (null arguments: skipped)

@@ -307,6 +307,16 @@ ASKJA_API int askja_batch_plaquette(askja_batch* b, double* out);
  *  - Errors are reported through askja_last_error(NULL). */
 ASKJA_API int askja_plaqexp_static(const askja_params* p, const void* links, double* out, void* stream);
 
+/* ---- domain decomposition (not in the reference) ------------------------ */
+/* Restricts the plaquette and link sums (askja_EnergyMag, askja_PlaqExp,
+ * askja_simpleenergyEl, askja_EnergyEl, askja_UViol, and the Hamiltonian of
+ * askja_trajectory) to the sites [s0, s1) of this context's lattice (site
+ * order of the U-conf layout, x0 slowest), 0 <= s0 < s1 <= V.  A rank that
+ * holds one x0 slab of a larger lattice plus halo slabs (askja_b200/slabs.py)
+ * counts only the slab it owns; the sums of all ranks then add up to the
+ * whole lattice's.  Default: every site. */
+ASKJA_API int askja_set_reduction_range(askja_ctx* ctx, long s0, long s1);
+
 /* ---- diagnostics (not in the reference) -------------------------------- */
 /* Exercises the tensor-core path's bounded wait (context on the tensor-core
  * mapping, kernel path 2, only): one CTA sets up as the tensor-core link update

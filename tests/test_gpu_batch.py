@@ -1,9 +1,8 @@
 """Batched uneven chains (askja_batch_*): every chain of a mixed batch must
 follow exactly the trajectory the same chain follows alone in the
 single-chain engine (same links, seed, BETA, DT, LEVEL): the batched kernels
-run the same per-link code, only the work distribution differs.  The batch's
-FP32 storage has no residual planes, so its single-chain twin is the
-"fp32-lean" engine."""
+run the same per-link code, only the work distribution differs (FP32 chains
+with NC <= 4 in the residual-plane mode, as a single FP32 chain)."""
 import numpy as np
 import pytest
 
@@ -30,9 +29,8 @@ def test_batch_matches_single_chains(precision):
         res = b.run(ntraj, nsteps, use_graph=True)
         ends = [b.get_links(c) for c in range(len(CHAINS))]
         plaq = b.plaquette()
-    single = "fp32-lean" if precision == "fp32" else precision
     for c, ch in enumerate(CHAINS):
-        with ab.Engine(ch["nc"], ch["dims"], beta=ch["beta"], dt=ch["dt"], level=ch["level"], precision=single,
+        with ab.Engine(ch["nc"], ch["dims"], beta=ch["beta"], dt=ch["dt"], level=ch["level"], precision=precision,
                        seed=ch["seed"]) as e:
             e.set_links(starts[c])
             last, _ = e.run_trajectories(ntraj, nsteps, use_graph=True)
