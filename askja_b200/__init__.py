@@ -42,7 +42,7 @@ EXPORTS = [
     "askja_GaussLaw", "askja_UViol", "askja_WilsonLoop", "askja_PolyakovLoop", "askja_WilsonLoopDir",
     "askja_PlaqExp", "askja_scalarLoopcorr", "askja_eigenphases", "askja_trajectory", "askja_run_trajectories", "askja_leapfrog",
     "askja_md_steps", "askja_params_load", "askja_params_store", "askja_file_stem", "askja_conf_write",
-    "askja_conf_read", "askja_host_alloc", "askja_host_free", "askja_plaqexp_static", "askja_tc_wait_selftest", "askja_set_reduction_range",
+    "askja_conf_read", "askja_host_alloc", "askja_host_free", "askja_plaqexp_static", "askja_tc_wait_selftest", "askja_set_reduction_range", "askja_slab",
     "askja_batch_create", "askja_batch_destroy", "askja_batch_last_error", "askja_batch_stream",
     "askja_batch_hot_start", "askja_batch_set_links", "askja_batch_get_links", "askja_batch_run",
     "askja_batch_plaquette", "askja_autotune", "askja_set_tuning", "askja_set_links_async", "askja_trajectory_async",
@@ -141,6 +141,7 @@ def library() -> ctypes.CDLL:
     L.askja_md_steps.argtypes = [vp, ip, ctypes.c_double]
     L.askja_tc_wait_selftest.argtypes = [vp, ctypes.c_longlong]
     L.askja_set_reduction_range.argtypes = [vp, ctypes.c_long, ctypes.c_long]
+    L.askja_slab.argtypes = [vp, ctypes.c_long, ctypes.c_long, vp, ip]
     L.askja_params_load.argtypes = [ctypes.c_char_p, ctypes.POINTER(RunParams)]
     L.askja_params_store.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(RunParams), ip, ip]
     L.askja_file_stem.argtypes = [ctypes.POINTER(RunParams), ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
@@ -220,6 +221,21 @@ class Engine:
     def set_reduction_range(self, s0: int, s1: int):
         """askja_set_reduction_range: only sites [s0, s1) enter the sums."""
         self._ck(self.lib.askja_set_reduction_range(self._ctx, int(s0), int(s1)))
+
+    def get_slab(self, s0: int, nsites: int) -> np.ndarray:
+        """askja_slab to host: links of sites [s0, s0 + nsites), U-conf layout."""
+        out = np.empty((nsites, self.dim, self.nc, self.nc), np.complex128)
+        self._ck(self.lib.askja_slab(self._ctx, int(s0), int(nsites), out.ctypes.data, 1))
+        return out
+
+    def set_slab(self, s0: int, links) -> None:
+        """askja_slab from host: links of sites [s0, s0 + len(links))."""
+        a = np.ascontiguousarray(links, dtype=np.complex128).reshape(-1, self.dim, self.nc, self.nc)
+        self._ck(self.lib.askja_slab(self._ctx, int(s0), a.shape[0], a.ctypes.data, 0))
+
+    def slab_device(self, s0: int, nsites: int, ptr: int, to_buf: bool) -> None:
+        """askja_slab with a device buffer (e.g. a torch CUDA tensor's data_ptr)."""
+        self._ck(self.lib.askja_slab(self._ctx, int(s0), int(nsites), int(ptr), 1 if to_buf else 0))
 
     def tc_wait_selftest(self, cycles: int):
         """askja_tc_wait_selftest: enqueue the tensor-core path's bounded wait

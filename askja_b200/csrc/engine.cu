@@ -1196,6 +1196,25 @@ int askja_set_reduction_range(askja_ctx* c, long s0, long s1) {
   return ASKJA_OK;
 }
 
+int askja_slab(askja_ctx* c, long s0, long nsites, double* buf, int to_buf) {
+  if (int rc = check_ctx(c)) return rc;
+  if (!buf || s0 < 0 || nsites < 1 || s0 + nsites > c->V) return set_err(c, ASKJA_ERR_ARG, "bad slab");
+  Range range("askja_slab");
+  DevGuard g(c->p.device);
+  const size_t bytes = (size_t)nsites * c->D * c->N * c->N * 2 * sizeof(double);
+  const bool fp64 = c->p.precision == ASKJA_FP64;
+  void* lo = c->split ? cur_ul(c) : nullptr;
+  if (to_buf) {
+    KL(askja::splitk::slab(c->lc, fp64, cur_u(c), lo, s0, nsites, c->staging, true), "slab");
+    CK(cudaMemcpyAsync(buf, c->staging, bytes, cudaMemcpyDefault, c->stream));
+  } else {
+    CK(cudaMemcpyAsync(c->staging, buf, bytes, cudaMemcpyDefault, c->stream));
+    KL(askja::splitk::slab(c->lc, fp64, cur_u(c), lo, s0, nsites, c->staging, false), "slab");
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  return ASKJA_OK;
+}
+
 int askja_tc_wait_selftest(askja_ctx* c, long long cycles) {
   if (int rc = check_ctx(c)) return rc;
   if (c->lc.force_rows != 2) return set_err(c, ASKJA_ERR_ARG, "the bounded-wait self-test needs the tensor-core path");

@@ -163,5 +163,26 @@ cudaError_t momenta_to_matrix(const LaunchCtx& c, const void* P, const void* PL,
   });
 }
 
+cudaError_t slab(const LaunchCtx& c, bool fp64, void* f, void* lo, long s0, long ns, void* buf, bool to_buf) {
+  const long tot = ns * c.lat.D * c.lat.N * c.lat.N;
+  const unsigned grid = blocks_for(tot, 256);
+  if (fp64) {
+    if (to_buf)
+      split::k_slab_get<double2><<<grid, 256, 0, c.stream>>>(c.lat, (const double2*)f, nullptr, (int)s0, (int)ns,
+                                                             (double2*)buf);
+    else
+      split::k_slab_set<double2><<<grid, 256, 0, c.stream>>>(c.lat, (double2*)f, nullptr, (int)s0, (int)ns,
+                                                             (const double2*)buf);
+  } else {
+    if (to_buf)
+      split::k_slab_get<float2><<<grid, 256, 0, c.stream>>>(c.lat, (const float2*)f, (const uint32_t*)lo, (int)s0,
+                                                            (int)ns, (double2*)buf);
+    else
+      split::k_slab_set<float2><<<grid, 256, 0, c.stream>>>(c.lat, (float2*)f, (uint32_t*)lo, (int)s0, (int)ns,
+                                                            (const double2*)buf);
+  }
+  return cudaGetLastError();
+}
+
 }  // namespace splitk
 }  // namespace askja

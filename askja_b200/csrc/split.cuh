@@ -759,5 +759,53 @@ __global__ void k_momenta_to_matrix(Lat L, const float* __restrict__ P, const ui
   small::store(F, Mf, L, d, s);
 }
 
+// ---- slabs of sites in the U-conf layout ----------------------------------------
+// Links of the sites [s0, s0 + ns) to / from buf in the U-conf order (FP64,
+// element t = ((s - s0) D + d) NN + e), for any storage: S2 = double2 or float2,
+// with the residual plane `lo` when non-null.  Used for the halo slabs of a
+// domain-decomposed chain.
+template <typename S2>
+__global__ void k_slab_get(Lat L, const S2* __restrict__ f, const uint32_t* __restrict__ lo, int s0, int ns,
+                           double2* __restrict__ buf) {
+  const int NN = L.N * L.N;
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long)ns * L.D * NN) return;
+  const long lk = t / NN;
+  const int e = (int)(t - lk * NN);
+  const int s = s0 + (int)(lk / L.D);
+  const int d = (int)(lk - (lk / L.D) * L.D);
+  const size_t o = eoff(L, d, e, s);
+  cpx<double> v = ldc<double>(f + o);
+  if (lo) {
+    const uint32_t w = lo[o];
+    v.re += (double)lo_low(w);
+    v.im += (double)lo_high(w);
+  }
+  buf[t] = make_double2(v.re, v.im);
+}
+
+template <typename S2>
+__global__ void k_slab_set(Lat L, S2* __restrict__ f, uint32_t* __restrict__ lo, int s0, int ns,
+                           const double2* __restrict__ buf) {
+  const int NN = L.N * L.N;
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long)ns * L.D * NN) return;
+  const long lk = t / NN;
+  const int e = (int)(t - lk * NN);
+  const int s = s0 + (int)(lk / L.D);
+  const int d = (int)(lk - (lk / L.D) * L.D);
+  const size_t o = eoff(L, d, e, s);
+  const double2 v = buf[t];
+  if (lo) {
+    float hr, lr, hi, li;
+    split_of(v.x, hr, lr);
+    split_of(v.y, hi, li);
+    stc(f + o, mkc<float>(hr, hi));
+    lo[o] = lo_pack(lr, li);
+  } else {
+    stc(f + o, mkc<double>(v.x, v.y));
+  }
+}
+
 }  // namespace split
 }  // namespace askja

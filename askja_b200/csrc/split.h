@@ -39,6 +39,10 @@ cudaError_t links_from_conf(const LaunchCtx& c, const void* conf, void* U, void*
 cudaError_t links_to_conf(const LaunchCtx& c, const void* U, const void* UL, void* conf);
 cudaError_t momenta_from_conf(const LaunchCtx& c, const void* conf, void* P, void* PL);
 cudaError_t momenta_to_conf(const LaunchCtx& c, const void* P, const void* PL, void* conf);
+// links of the sites [s0, s0 + ns) to (to_buf) or from device memory buf in the
+// U-conf order (FP64); any storage: FP64 (fp64), FP32 with (lo non-null) or
+// without residual plane
+cudaError_t slab(const LaunchCtx& c, bool fp64, void* f, void* lo, long s0, long ns, void* buf, bool to_buf);
 // full FP32 matrices in the float2 field layout (for the matrix diagnostics)
 cudaError_t momenta_to_matrix(const LaunchCtx& c, const void* P, const void* PL, void* F);
 

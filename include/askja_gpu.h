@@ -316,6 +316,13 @@ ASKJA_API int askja_plaqexp_static(const askja_params* p, const void* links, dou
  * counts only the slab it owns; the sums of all ranks then add up to the
  * whole lattice's.  Default: every site. */
 ASKJA_API int askja_set_reduction_range(askja_ctx* ctx, long s0, long s1);
+/* Current links of the sites [s0, s0 + nsites) copied to (to_buf = 1) or from
+ * (to_buf = 0) buf in the U-conf order ([site][dir][row][col][re,im] doubles,
+ * nsites * DIM * NC * NC * 2 of them); buf may be host or device memory.
+ * Returns when the copy is complete.  With x0 slowest, one x0 slab is the
+ * nsites = V / N0 sites from s0 = x0 * V / N0: the halo exchange of a
+ * domain-decomposed chain. */
+ASKJA_API int askja_slab(askja_ctx* ctx, long s0, long nsites, double* buf, int to_buf);
 
 /* ---- diagnostics (not in the reference) -------------------------------- */
 /* Exercises the tensor-core path's bounded wait (context on the tensor-core
