@@ -417,10 +417,10 @@ __device__ __forceinline__ void link_update(const Lat& L, const float2* __restri
   }
 }
 
-// Register budget: OCC 0 the compiler's choice, 1 / 2 bounded for 6 / 7
-// resident CTAs of 128 threads per SM.
+// Register budget: at most 128 registers (4 resident CTAs of 128 threads per
+// SM) for OCC 0, bounded for 6 / 7 resident CTAs for OCC 1 / 2.
 template <int N, int MODE, int OCC>
-__global__ void __launch_bounds__(128, OCC == 0 ? 1 : 5 + OCC)
+__global__ void __launch_bounds__(128, OCC == 0 ? 4 : 5 + OCC)
     k_force(Lat L, const float2* __restrict__ U, const uint32_t* __restrict__ UL, const float* Pin,
             const uint32_t* PLin, float* Pout, uint32_t* PLout, float2* __restrict__ Uout,
             uint32_t* __restrict__ ULout, float eps_k, float eps_d, int order) {
