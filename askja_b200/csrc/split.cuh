@@ -268,37 +268,44 @@ __device__ __forceinline__ void exp_minus_one(small::Mat<N, float>& E, const sma
     det = fmaf(-p1, n02, det);
     det = fmaf(-p2, n01, det);
     det = fmaf(2.f, re3, det);
-    const float tau = eps * trp;
-    const float c1 = 0.5f * fmaf(eps * eps, trq, -tau * tau);
-    const float dd = -(eps * eps * eps) * det;
-    float a = 1.f, b = 0.f, g = 0.f, f = 1.f;
-    cpx<float> A = czero<float>(), B = czero<float>(), C = czero<float>();
+    // The scalar series runs in FP64.  In FP32 the P^2 coefficient would carry
+    // fl(eps^2) while the P coefficient carries eps: that rounding is the same
+    // for every link, so E would miss unitarity by the fixed amount
+    // (eps^2 - fl(eps^2)) P^2 at every update, and the link norms -- hence
+    // the action -- would drift in one direction (about +0.04 in dH per
+    // 50-step trajectory at SU(3) 32^4).  From FP64 coefficients each FP32
+    // rounding is link-dependent and the remaining error averages out.
+    const double e1 = (double)eps;
+    const double tau = e1 * (double)trp;
+    const double c1 = 0.5 * fma(e1 * e1, (double)trq, -tau * tau);
+    const double dd = -(e1 * e1 * e1) * (double)det;
+    double a = 1.0, b = 0.0, g = 0.0, f = 1.0;
+    double Ar = 0.0, Ai = 0.0, Br = 0.0, Bi = 0.0, Cr = 0.0, Ci = 0.0;
 #pragma unroll
     for (int k = 1; k <= 8; k++) {
       if (k > order) break;
-      const float na = -dd * g;
-      const float nb = fmaf(c1, g, a);
-      const float ng = fmaf(tau, g, b);
+      const double na = -dd * g;
+      const double nb = fma(c1, g, a);
+      const double ng = fma(tau, g, b);
       a = na;
       b = nb;
       g = ng;
-      f = f * (1.f / k);
-      const float sf = (k & 2) ? -f : f;
+      f = f * (1.0 / k);
+      const double sf = (k & 2) ? -f : f;
       if (k & 1) {
-        A.im = fmaf(sf, a, A.im);
-        B.im = fmaf(sf, b, B.im);
-        C.im = fmaf(sf, g, C.im);
+        Ai = fma(sf, a, Ai);
+        Bi = fma(sf, b, Bi);
+        Ci = fma(sf, g, Ci);
       } else {
-        A.re = fmaf(sf, a, A.re);
-        B.re = fmaf(sf, b, B.re);
-        C.re = fmaf(sf, g, C.re);
+        Ar = fma(sf, a, Ar);
+        Br = fma(sf, b, Br);
+        Cr = fma(sf, g, Cr);
       }
     }
-    B.re *= eps;
-    B.im *= eps;
-    const float e2 = eps * eps;
-    C.re *= e2;
-    C.im *= e2;
+    const double e2 = e1 * e1;
+    const cpx<float> A = mkc<float>((float)Ar, (float)Ai);
+    const cpx<float> B = mkc<float>((float)(Br * e1), (float)(Bi * e1));
+    const cpx<float> C = mkc<float>((float)(Cr * e2), (float)(Ci * e2));
     const float pd[3] = {p0, p1, p2}, qd[3] = {q0, q1, q2};
 #pragma unroll
     for (int i = 0; i < 3; i++) {

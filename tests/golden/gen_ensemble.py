@@ -2,10 +2,15 @@
 run of the reference itself.
 
 The reference's own askja (sun.cpp compiled unchanged against the project's
-GSL shim into oracle/_ref/askja_ref by oracle/Makefile) runs an SU(3) 4^4 HMC
-chain from a cold start: BETA 5.70, DT 0.02, LEVEL 8, UPDATE2 50 (50 MD steps
-per trajectory), 2000 trajectories, a configuration stored after every
-trajectory.  The reference's own measure4d (oracle/_ref/measure4d_ref) then
+GSL shim by oracle/Makefile, as oracle/_ref/askja_ref_clock: its time() is a
+counter that advances on every call) runs an SU(3) 4^4 HMC chain from a cold
+start: BETA 5.70, DT 0.02, LEVEL 8, UPDATE2 50 (50 MD steps per trajectory),
+4000 trajectories, a configuration stored after every trajectory.  The
+reference reseeds its generator from time(NULL) for every momentum refresh and
+every Metropolis uniform (sun.cpp:1268-1311); with the wall clock, the ~20
+trajectories it runs per second here would share seeds -- the same momenta and
+uniforms -- and the chain would sample a biased ensemble (a first fixture made
+that way had a Polyakov loop 2-4 sigma below two independent GPU runs).  The reference's own measure4d (oracle/_ref/measure4d_ref) then
 measures the stored configurations after SKIP thermalisation ones and writes
 its Nrav line (<|P|>, <W>, beta/N0 <plaquette> temporal and spatial, each with
 the reference's naive error).  The same per-configuration observables are
@@ -14,7 +19,7 @@ stored as means over bins of BIN consecutive configurations, from which the
 test forms errors that include the autocorrelation.
 
 Needs oracle/_ref (built where the reference sources are); never runs on the
-GPU host.  Takes about three minutes on 8 cores.
+GPU host.  Takes about seven minutes on 8 cores.
 
     python tests/golden/gen_ensemble.py
 """
@@ -36,7 +41,7 @@ from oracle import REF_DIR, Reference  # noqa: E402
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "ensemble_su3_4x4x4x4.json")
 
 NC, DIMS, BETA, DT, LEVEL, UPDATE2 = 3, [4, 4, 4, 4], 5.70, 0.02, 8, 50
-NTRAJ, SKIP, BIN = 2000, 100, 25
+NTRAJ, SKIP, BIN = 4000, 200, 100
 
 PARAMS = """#Parameters_file
 NC              {nc}
@@ -70,7 +75,7 @@ def main():
     with open(os.path.join(work, "p.txt"), "w") as f:
         f.write(params_text(NTRAJ))
     env = dict(os.environ, OMP_NUM_THREADS=str(os.cpu_count() or 1))
-    r = subprocess.run([os.path.join(REF_DIR, "askja_ref"), "p.txt"], cwd=work, env=env, capture_output=True,
+    r = subprocess.run([os.path.join(REF_DIR, "askja_ref_clock"), "p.txt"], cwd=work, env=env, capture_output=True,
                        text=True)
     assert r.returncode == 0 and "Finished successfully" in r.stdout, r.stdout[-2000:]
     acc_line = [ln for ln in r.stdout.splitlines() if "Statistics" in ln][-1]
@@ -95,7 +100,7 @@ def main():
     nb = (taken - SKIP) // BIN
     bins = {k: np.asarray(v[:nb * BIN]).reshape(nb, BIN).mean(axis=1).tolist() for k, v in series.items()}
     fixture = {
-        "generator": "tests/golden/gen_ensemble.py: oracle/_ref/askja_ref + oracle/_ref/measure4d_ref",
+        "generator": "tests/golden/gen_ensemble.py: oracle/_ref/askja_ref_clock + oracle/_ref/measure4d_ref",
         "params": {"nc": NC, "dims": DIMS, "beta": BETA, "dt": DT, "level": LEVEL, "update2": UPDATE2,
                    "trajectories": NTRAJ, "conftake": 1, "random": 0},
         "reference_acceptance": acc_line.strip(),

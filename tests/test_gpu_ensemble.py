@@ -2,14 +2,15 @@
 
 tests/golden/ensemble_su3_4x4x4x4.json holds what the reference's own askja
 and measure4d produced for an SU(3) 4^4 chain (BETA 5.70, DT 0.02, LEVEL 8,
-50 MD steps per trajectory, 2000 trajectories from a cold start; made by
+50 MD steps per trajectory, 4000 trajectories from a cold start; made by
 tests/golden/gen_ensemble.py).  Here the GPU askja CLI runs the same params
 file in FP64 and in FP32-mixed, the GPU measure4d measures its configurations
 with the same SKIP, and the ensemble averages of the plaquettes (temporal and
 spatial, beta/N0 normalised as in the Nrav file) and of the Polyakov loop
 must agree with the reference's within 2 sigma.  Sigma combines both chains'
-errors of the mean from bins of 25 consecutive configurations (the Nrav
-errors of measure4d ignore the autocorrelation).  The two chains draw
+errors of the mean from bins of 100 consecutive configurations (the Nrav
+errors of measure4d ignore the autocorrelation, which at this coupling --
+near the N0 = 4 deconfinement transition -- is long for the Polyakov loop).  The two chains draw
 different random numbers (the reference's GSL stream is not reproducible),
 so this is a statistical comparison; the engine is deterministic for a fixed
 seed (RANDOM 0), so the outcome is too."""

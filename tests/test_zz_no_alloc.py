@@ -31,11 +31,15 @@ def test_static_plaqexp_matches_plaqexp(precision, nc, dims):
     lib.askja_plaqexp_static.argtypes = [ctypes.POINTER(ab.Params), ctypes.c_void_p, ctypes.c_void_p,
                                          ctypes.c_void_p]
     lib.askja_plaqexp_static.restype = ctypes.c_int
-    with ab.Engine(nc, dims, beta=5.0, precision=precision) as e:
+    # the entry point reads plain FP32 links, so its FP32 counterpart is an
+    # engine holding exactly those (the FP32-only storage, no residual plane)
+    engine_precision = "fp32-lean" if precision == "fp32" else precision
+    with ab.Engine(nc, dims, beta=5.0, precision=engine_precision) as e:
         e.hot_start(11)
         want = np.array(e.PlaqExp())
         u = e.get_links()
         params = e.params
+    params.precision = ab.FP32 if precision == "fp32" else ab.FP64  # the entry point's link storage
     links = torch.from_numpy(_soa(u, precision).view(np.float32 if precision == "fp32" else np.float64)).cuda()
     out = torch.full((2,), float("nan"), dtype=torch.float64, device="cuda")
     stream = torch.cuda.current_stream().cuda_stream
