@@ -174,12 +174,17 @@ __device__ __forceinline__ void force_coefs(float (&f)[Dims<N>::NCOEF], const sm
       f[2 * p] = 0.5f * (W.a[i][j].im + W.a[j][i].im);
       f[2 * p + 1] = -0.5f * (W.a[i][j].re - W.a[j][i].re);
     }
-  float trim = 0.f;
+  // The trace is taken out in FP64.  Only the first N-1 diagonal entries are
+  // kept (the last is minus their sum), so the last one's force is implied
+  // as -(F_00 + ... ); an FP32 trace times fl(1/N) would give every link the
+  // same relative error in that implied entry, an error along the diagonal
+  // generator that correlates with the momentum and drifts the energy.
+  double tr = 0.0;
 #pragma unroll
-  for (int k = 0; k < N; k++) trim += W.a[k][k].im;
-  trim *= 1.f / N;
+  for (int k = 0; k < N; k++) tr += (double)W.a[k][k].im;
+  tr /= N;
 #pragma unroll
-  for (int m = 0; m < N - 1; m++) f[Dims<N>::NDIAG + m] = W.a[m][m].im - trim;
+  for (int m = 0; m < N - 1; m++) f[Dims<N>::NDIAG + m] = (float)((double)W.a[m][m].im - tr);
 }
 
 // ---- links -----------------------------------------------------------------
@@ -330,26 +335,36 @@ __device__ __forceinline__ void exp_minus_one(small::Mat<N, float>& E, const sma
     for (int i = 0; i < 2; i++)
 #pragma unroll
       for (int j = 0; j < 2; j++) X.a[i][j] = mkc<float>(-eps * P.a[i][j].im, eps * P.a[i][j].re);
-    const cpx<float> tr = mkc<float>(X.a[0][0].re + X.a[1][1].re, X.a[0][0].im + X.a[1][1].im);
-    cpx<float> d = small::cmul(X.a[0][0], X.a[1][1]);
-    cmsub(d, X.a[0][1], X.a[1][0]);
-    cpx<float> al = mkc<float>(1.f, 0.f), be = czero<float>();
-    cpx<float> sa = czero<float>(), sb = czero<float>();  // the X^0 term is left out: E - 1
-    float f = 1.f;
+    // tr X and det X of the FP32 X, then the scalar series in FP64: summed in
+    // FP32, its small high-order terms (d^2/120 ~ 1e-8 added to ~1) would be
+    // rounded away in every link the same way, and E would lose norm on
+    // average (~4e-12 per update at |X|^2 ~ 1e-3), an energy drift.
+    const double trr = (double)X.a[0][0].re + (double)X.a[1][1].re;
+    const double tri = (double)X.a[0][0].im + (double)X.a[1][1].im;
+    const double dr = (double)X.a[0][0].re * X.a[1][1].re - (double)X.a[0][0].im * X.a[1][1].im -
+                      ((double)X.a[0][1].re * X.a[1][0].re - (double)X.a[0][1].im * X.a[1][0].im);
+    const double di = (double)X.a[0][0].re * X.a[1][1].im + (double)X.a[0][0].im * X.a[1][1].re -
+                      ((double)X.a[0][1].re * X.a[1][0].im + (double)X.a[0][1].im * X.a[1][0].re);
+    double alr = 1.0, ali = 0.0, ber = 0.0, bei = 0.0;
+    double sar = 0.0, sai = 0.0, sbr = 0.0, sbi = 0.0;  // the X^0 term is left out: E - 1
+    double f = 1.0;
 #pragma unroll
     for (int k = 1; k <= 8; k++) {
       if (k > order) break;
-      cpx<float> nal = czero<float>(), nbe = al;
-      cmsub(nal, be, d);
-      cmac(nbe, be, tr);
-      al = nal;
-      be = nbe;
-      f = f * (1.f / k);
-      sa.re = fmaf(f, al.re, sa.re);
-      sa.im = fmaf(f, al.im, sa.im);
-      sb.re = fmaf(f, be.re, sb.re);
-      sb.im = fmaf(f, be.im, sb.im);
+      // X^k = -be_{k-1} det 1 + (al_{k-1} + be_{k-1} tr) X
+      const double nalr = -(ber * dr - bei * di), nali = -(ber * di + bei * dr);
+      const double nber = alr + (ber * trr - bei * tri), nbei = ali + (ber * tri + bei * trr);
+      alr = nalr;
+      ali = nali;
+      ber = nber;
+      bei = nbei;
+      f = f * (1.0 / k);
+      sar = fma(f, alr, sar);
+      sai = fma(f, ali, sai);
+      sbr = fma(f, ber, sbr);
+      sbi = fma(f, bei, sbi);
     }
+    const cpx<float> sa = mkc<float>((float)sar, (float)sai), sb = mkc<float>((float)sbr, (float)sbi);
 #pragma unroll
     for (int i = 0; i < 2; i++)
 #pragma unroll

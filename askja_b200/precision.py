@@ -69,12 +69,15 @@ def compare(nc, dims, beta, dt, level, nsteps, u0, ntraj_dh=3, seed=7, device=0,
             p = e64.get_momenta(0)
             e32.set_links(u0)
             e32.set_momenta(p, 0)
-            h = []
+            h, ds = [], []
             for e in (e64, e32):
-                h0 = e.hamiltonian(0)
+                h0, s0 = e.hamiltonian(0), e.EnergyMag()
                 e.leapfrog(nsteps, dt)
                 h.append(e.hamiltonian(0) - h0)
-            rows.append({"dH64": h[0], "dH32": h[1], "abs_diff": abs(h[1] - h[0])})
+                ds.append(beta * (e.EnergyMag() - s0))
+            # dS64: the trajectory's change of the action (a relative bias c of
+            # the FP32 force shows up as dH32 - dH64 ~ c dS)
+            rows.append({"dH64": h[0], "dH32": h[1], "abs_diff": abs(h[1] - h[0]), "dS64": ds[0]})
             if t == 0:
                 u32 = e32.get_links().reshape(-1, nc, nc)
                 out["unitarity_max"] = float(np.abs(np.einsum("lij,lkj->lik", u32, u32.conj()) - np.eye(nc)).max())

@@ -447,7 +447,7 @@ def precision_report(cfg, dev):
     reversibility and unitarity (askja_b200.precision)."""
     from askja_b200 import precision
     nc, dims = cfg["nc"], cfg["dims"]
-    therm = 50
+    therm = 200
     u0 = precision.thermalise(nc, dims, cfg["beta"], cfg["dt"], cfg["level"], cfg["nsteps"], therm, 4242, dev)
     r = precision.compare(nc, dims, cfg["beta"], cfg["dt"], cfg["level"], cfg["nsteps"], u0, ntraj_dh=3,
                           device=dev)

@@ -5,7 +5,7 @@ The reference's own askja (sun.cpp compiled unchanged against the project's
 GSL shim by oracle/Makefile, as oracle/_ref/askja_ref_clock: its time() is a
 counter that advances on every call) runs an SU(3) 4^4 HMC chain from a cold
 start: BETA 5.70, DT 0.02, LEVEL 8, UPDATE2 50 (50 MD steps per trajectory),
-4000 trajectories, a configuration stored after every trajectory.  The
+16000 trajectories, a configuration stored after every trajectory.  The
 reference reseeds its generator from time(NULL) for every momentum refresh and
 every Metropolis uniform (sun.cpp:1268-1311); with the wall clock, the ~20
 trajectories it runs per second here would share seeds -- the same momenta and
@@ -19,7 +19,7 @@ stored as means over bins of BIN consecutive configurations, from which the
 test forms errors that include the autocorrelation.
 
 Needs oracle/_ref (built where the reference sources are); never runs on the
-GPU host.  Takes about seven minutes on 8 cores.
+GPU host.  Takes about half an hour on 8 cores.
 
     python tests/golden/gen_ensemble.py
 """
@@ -41,7 +41,7 @@ from oracle import REF_DIR, Reference  # noqa: E402
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "ensemble_su3_4x4x4x4.json")
 
 NC, DIMS, BETA, DT, LEVEL, UPDATE2 = 3, [4, 4, 4, 4], 5.70, 0.02, 8, 50
-NTRAJ, SKIP, BIN = 4000, 200, 100
+NTRAJ, SKIP, BIN = 16000, 400, 200
 
 PARAMS = """#Parameters_file
 NC              {nc}
