@@ -759,7 +759,7 @@ def main():
     ap.add_argument("--no-precision", action="store_true")
     ap.add_argument("--kernel-only", action="store_true", help="fused-kernel microbenchmark (profiling)")
     ap.add_argument("--no-tune", action="store_true", help="default kernel mapping, no autotuning")
-    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"], help="with --kernel-only")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp32-lean", "fp64"], help="with --kernel-only")
     ap.add_argument("--path", type=int, default=0, help="with --kernel-only: askja kernel_path")
     ap.add_argument("--occ", type=int, default=0, help="with --kernel-only: register budget (askja_tuning.occupancy)")
     args = ap.parse_args()
