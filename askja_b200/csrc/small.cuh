@@ -405,24 +405,39 @@ __device__ __forceinline__ void expi_times_herm3(Mat<3, T>& Tm, const Mat<3, T>&
   const T e2 = eps * eps;
   C.re *= e2;
   C.im *= e2;
+  // Each entry is summed from its smallest term up and ends on its largest, so
+  // that terms below half an ulp of the entry (C.im, A.im) are rounded with
+  // it instead of being dropped: dropped, they take away a (det P)^2 part of
+  // unitarity and every update shrinks the link a little.
   Mat<3, T> E;
   const T pd[3] = {p0, p1, p2}, qd[3] = {q0, q1, q2};
 #pragma unroll
   for (int i = 0; i < 3; i++) {
     E.a[i][i].re = fma(C.re, qd[i], fma(B.re, pd[i], A.re));
-    E.a[i][i].im = fma(C.im, qd[i], fma(B.im, pd[i], A.im));
+    E.a[i][i].im = fma(B.im, pd[i], fma(C.im, qd[i], A.im));
   }
   const cpx<T> Qu[3] = {Q01, Q02, Q12};
   const int iu[3] = {0, 0, 1}, ju[3] = {1, 2, 2};
 #pragma unroll
   for (int u = 0; u < 3; u++) {
     const int i = iu[u], j = ju[u];
-    cpx<T> e = cmul(B, P.a[i][j]);  // upper: B P_ij + C Q_ij
-    cmac(e, C, Qu[u]);
-    E.a[i][j] = e;
-    cpx<T> l = cmul(B, P.a[j][i]);  // lower: B P_ji + C conj(Q_ij)
-    cmac_nc(l, C, Qu[u]);
-    E.a[j][i] = l;
+    const cpx<T> q = Qu[u], pu = P.a[i][j], pl = P.a[j][i];
+    // upper: B P_ij + C Q_ij
+    T r = fma(B.re, pu.re, -(C.im * q.im));
+    r = fma(C.re, q.re, r);
+    r = fma(-B.im, pu.im, r);
+    T m = fma(B.re, pu.im, C.im * q.re);
+    m = fma(C.re, q.im, m);
+    m = fma(B.im, pu.re, m);
+    E.a[i][j] = mkc<T>(r, m);
+    // lower: B P_ji + C conj(Q_ij)
+    r = fma(B.re, pl.re, C.im * q.im);
+    r = fma(C.re, q.re, r);
+    r = fma(-B.im, pl.im, r);
+    m = fma(B.re, pl.im, C.im * q.re);
+    m = fma(-C.re, q.im, m);
+    m = fma(B.im, pl.re, m);
+    E.a[j][i] = mkc<T>(r, m);
   }
   Tm = Ux;
   mac_nn(Tm, E, Ux);
