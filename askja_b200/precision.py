@@ -34,9 +34,11 @@ def _binned_error(x: np.ndarray, nbins: int = 10) -> float:
     return float(b.std(ddof=1) / np.sqrt(nbins))
 
 
-def thermalise(nc, dims, beta, dt, level, nsteps, ntraj, seed, device=0, reunitarise=None, kernel_path=0):
-    """Hot start, then `ntraj` FP32-mixed trajectories; returns FP64 U-conf links."""
-    with Engine(nc, dims, beta=beta, dt=dt, level=level, precision="fp32", device=device, seed=seed,
+def thermalise(nc, dims, beta, dt, level, nsteps, ntraj, seed, device=0, reunitarise=None, kernel_path=0,
+               fp32="fp32"):
+    """Hot start, then `ntraj` FP32-mixed trajectories (engine precision `fp32`:
+    "fp32" or "fp32-lean"); returns FP64 U-conf links."""
+    with Engine(nc, dims, beta=beta, dt=dt, level=level, precision=fp32, device=device, seed=seed,
                 reunitarise=reunitarise, kernel_path=kernel_path) as e:
         e.hot_start(seed + 1)
         if ntraj:
@@ -44,11 +46,12 @@ def thermalise(nc, dims, beta, dt, level, nsteps, ntraj, seed, device=0, reunita
         return e.get_links()
 
 
-def compare(nc, dims, beta, dt, level, nsteps, u0, ntraj_dh=3, seed=7, device=0, reunitarise=None, kernel_path=0):
+def compare(nc, dims, beta, dt, level, nsteps, u0, ntraj_dh=3, seed=7, device=0, reunitarise=None, kernel_path=0,
+            fp32="fp32"):
     out = {}
     kw = dict(beta=beta, dt=dt, level=level, device=device)
     with Engine(nc, dims, precision="fp64", seed=seed, **kw) as e64, \
-            Engine(nc, dims, precision="fp32", seed=seed, reunitarise=reunitarise, kernel_path=kernel_path,
+            Engine(nc, dims, precision=fp32, seed=seed, reunitarise=reunitarise, kernel_path=kernel_path,
                    **kw) as e32:
         # one force evaluation on identical inputs
         e64.set_links(u0)
@@ -98,7 +101,8 @@ def compare(nc, dims, beta, dt, level, nsteps, u0, ntraj_dh=3, seed=7, device=0,
     return out
 
 
-def ensemble(nc, dims, beta, dt, level, nsteps, u0, ntraj, seed=11, device=0, reunitarise=None, kernel_path=0):
+def ensemble(nc, dims, beta, dt, level, nsteps, u0, ntraj, seed=11, device=0, reunitarise=None, kernel_path=0,
+             fp32="fp32"):
     res = {}
     vol = int(np.prod(dims))
     D = len(dims)
@@ -107,7 +111,8 @@ def ensemble(nc, dims, beta, dt, level, nsteps, u0, ntraj, seed=11, device=0, re
     obs = ("plaquette", "plaquette_t", "plaquette_s", "polyakov", "wilson")
     for prec in ("fp64", "fp32"):
         extra = dict(reunitarise=reunitarise, kernel_path=kernel_path) if prec == "fp32" else {}
-        with Engine(nc, dims, beta=beta, dt=dt, level=level, precision=prec, device=device, seed=seed, **extra) as e:
+        with Engine(nc, dims, beta=beta, dt=dt, level=level, precision=fp32 if prec == "fp32" else prec,
+                    device=device, seed=seed, **extra) as e:
             e.set_links(u0)
             series = {k: [] for k in obs}
             acc = 0
@@ -150,8 +155,11 @@ def main():
     ap.add_argument("--fp32-reunit", choices=["default", "on", "off"], default="default",
                     help="FP32 engines: per-update reunitarisation (default: on)")
     ap.add_argument("--fp32-path", type=int, default=0, help="FP32 engines: askja kernel_path")
+    ap.add_argument("--fp32-storage", choices=["residual", "lean"], default="residual",
+                    help="FP32 engines: FP32 + bfloat16 residual planes, or FP32-only storage")
     a = ap.parse_args()
-    kw = dict(reunitarise={"default": None, "on": True, "off": False}[a.fp32_reunit], kernel_path=a.fp32_path)
+    kw = dict(reunitarise={"default": None, "on": True, "off": False}[a.fp32_reunit], kernel_path=a.fp32_path,
+              fp32="fp32" if a.fp32_storage == "residual" else "fp32-lean")
     t0 = time.perf_counter()
     u0 = thermalise(a.nc, a.dims, a.beta, a.dt, a.level, a.nsteps, a.therm, a.seed, **kw)
     rep = {"config": vars(a), "therm_seconds": time.perf_counter() - t0}
