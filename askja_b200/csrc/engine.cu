@@ -1115,6 +1115,12 @@ int askja_autotune(askja_ctx* c, int reps, askja_tuning* out) {
     seen.push_back(eff);
     cands.push_back({1, eff, 0});
   }
+  // FP32 rows for 5 <= NC <= 8 (k_force8): tighter register budgets at the default sites per CTA
+  if (!c->split && !fp64 && c->N > 4 && c->N <= 8) {
+    const int eff = askja::rows_effective_groups(c->N, fp64, 0);
+    cands.push_back({1, eff, 1});
+    cands.push_back({1, eff, 2});
+  }
   if (cands.size() > 24) cands.resize(24);
   // scratch: Pi holds a copy of pi, the partner link buffer receives the output
   CK(cudaMemcpyAsync(c->P2, c->P, c->field_bytes, cudaMemcpyDeviceToDevice, c->stream));

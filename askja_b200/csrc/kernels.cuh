@@ -63,7 +63,8 @@ cudaError_t rows_force(const LaunchCtx& c, int mode, const void* U, const void* 
                                              c.order, c.reunit);
   } else {
     auto k = rows::k_force<NMAX, T, S2, 1>;
-    if constexpr (sizeof(T) == 4 && NMAX == 8) k = rows::k_force8<S2, 1>;
+    if constexpr (sizeof(T) == 4 && NMAX == 8)
+      k = c.small_occ == 2 ? rows::k_force8<S2, 1, 2> : c.small_occ == 1 ? rows::k_force8<S2, 1, 1> : rows::k_force8<S2, 1, 0>;
     if ((e = set_smem(k, smem)) != cudaSuccess) return e;
     // reunit 2: Newton-Schulz projection (FP32 single chains, see LaunchCtx::rows_ns)
     const int ru = (sizeof(T) == 4 && c.reunit && c.rows_ns) ? 2 : c.reunit;

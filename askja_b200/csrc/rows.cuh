@@ -565,9 +565,10 @@ __global__ void k_force(Lat L, const S2* __restrict__ U, const S2* Pin, S2* Pout
 }
 
 // The same for FP32 with NMAX = 8 (the Paterson-Stockmeyer drift): at most 128
-// registers, so that four 128-thread CTAs stay resident per SM.
-template <typename S2, int MODE>
-__global__ void __launch_bounds__(256, 2) k_force8(Lat L, const S2* __restrict__ U, const S2* Pin, S2* Pout,
+// registers, so that four 128-thread CTAs stay resident per SM (OCC 0), or
+// tighter budgets for six / eight (OCC 1 / 2).
+template <typename S2, int MODE, int OCC = 0>
+__global__ void __launch_bounds__(256, 2 + OCC) k_force8(Lat L, const S2* __restrict__ U, const S2* Pin, S2* Pout,
                                                    S2* __restrict__ Uout, float eps_k, float eps_d, int order,
                                                    int reunit) {
   extern __shared__ __align__(16) unsigned char smem_raw[];

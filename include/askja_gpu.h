@@ -232,7 +232,8 @@ ASKJA_API int askja_md_steps(askja_ctx* ctx, int nsteps, double eps);
 typedef struct {
   int path;       /* 0 thread-per-link, 1 row-per-thread, 2 tensor cores, 3 site pairs */
   int groups;     /* row-per-thread: sites per CTA (0 = default) */
-  int occupancy;  /* thread-per-link: 0 default registers, 1 and 2 tighter budgets / more resident CTAs */
+  int occupancy;  /* thread-per-link, and row-per-thread FP32 with 5 <= NC <= 8: 0 default registers, 1 and 2
+                     tighter budgets / more resident CTAs */
   int ncand;      /* candidates timed */
   double best_us; /* fused kick+drift launch time of the choice, microseconds */
   int cand_path[24], cand_groups[24], cand_occ[24];
