@@ -337,8 +337,12 @@ def run_ours(args):
     f32, f64 = res["fp32"], res["fp64"]
     hbm, peak_kind = peaks()
     residual = nc <= 4 and not cfg.get("tensor")  # the residual-plane FP32 mode
+    # algorithmic bytes of a link update: read U, read P, write P, write U as full
+    # NC x NC FP32 complex matrices, neighbour links as cache hits (4 NC^2 x 8 B);
+    # the residual planes' own layout moves link_update_bytes (312 B for SU(3))
+    alg_per_lu = 4 * nc * nc * 8
     bytes_per_lu = link_update_bytes(nc, residual)
-    achieved = bytes_per_lu * links / (f32["kernel_ms"] / 1e3) / 1e9
+    achieved = alg_per_lu * links / (f32["kernel_ms"] / 1e3) / 1e9
     traffic = measured_traffic(args.config)
     if cfg.get("tensor"):
         fpl = tensor_flops_per_link(nc, len(dims), cfg["level"])
@@ -378,7 +382,12 @@ def run_ours(args):
         roofline = {"bound": "hbm", "kernel": f"fused kick+drift ({kname})",
                     "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                     "peak_source": peak_kind, "traffic": None if paired else traffic,
-                    "bytes_per_launch": bytes_per_lu * links, "avg_launch_ms": f32["kernel_ms"],
+                    "bytes_per_launch": alg_per_lu * links, "avg_launch_ms": f32["kernel_ms"],
+                    "storage_bytes_per_launch": bytes_per_lu * links,
+                    "storage_achieved": bytes_per_lu * links / (f32["kernel_ms"] / 1e3) / 1e9,
+                    "storage_note": "compulsory bytes of the stored layout (FP32 links and momentum "
+                                    "coordinates with bfloat16 residual planes): the traffic to compare "
+                                    "`traffic` with",
                     "fp32": {"flops_per_launch": fpl * links, "achieved": tf32, "peak": pk32, "unit": "TFLOP/s",
                              "frac": tf32 / pk32,
                              "peak_source": "measured FFMA on this device (askja_peak_flops)",

@@ -46,3 +46,30 @@ def test_set_tuning_rejects_nonsense():
     with ab.Engine(8, [2, 2, 2], beta=1.0) as e:
         with pytest.raises(ab.AskjaError):
             ab.set_tuning(e, {"path": 0})  # thread-per-link does not exist for NC = 8
+
+
+@pytest.mark.parametrize("nc", [5, 8])
+def test_fp32_row_register_budgets_agree(nc):
+    """The FP32 row kernel for 5 <= NC <= 8 at its three register budgets
+    (occupancy 0, 1, 2: 128, 80 and 64 registers, the tighter ones spilling)
+    is the same code: identical fields after a few steps, and candidates of the
+    autotuner."""
+    dims = [3, 2, 4, 4]
+    rng = np.random.default_rng(40 + nc)
+    O = Oracle(nc, dims)
+    nl = O.vol * O.dim
+    u = fields.haar(nc, nl, rng).reshape(O.shape)
+    pi = fields.momenta(nc, nl, 2.0 * nc, rng, O)
+    out = []
+    with ab.Engine(nc, dims, beta=2.0 * nc, dt=0.01, level=8, precision="fp32") as e:
+        t = ab.autotune(e, reps=2)
+        assert {c["occupancy"] for c in t["candidates"] if c["path"] == 1} == {0, 1, 2}
+        for occ in (0, 1, 2):
+            ab.set_tuning(e, {"path": 1, "occupancy": occ})
+            e.set_links(u)
+            e.set_momenta(pi, 0)
+            e.leapfrog(3, 0.01)
+            out.append((e.get_links(), e.get_momenta(0)))
+    for links, mom in out[1:]:
+        np.testing.assert_array_equal(links, out[0][0])
+        np.testing.assert_array_equal(mom, out[0][1])
