@@ -581,8 +581,10 @@ __device__ __forceinline__ void plaq_site(const Lat& L, const float2* __restrict
   }
 }
 
+// At most 128 registers (two 256-thread CTAs per SM): unbounded, the four FP64
+// matrices took 172 and left one CTA per SM.
 template <int N>
-__global__ void __launch_bounds__(misc::RED_THREADS) k_plaq(Lat L, const float2* __restrict__ U,
+__global__ void __launch_bounds__(misc::RED_THREADS, 2) k_plaq(Lat L, const float2* __restrict__ U,
                                                             const uint32_t* __restrict__ UL,
                                                             double* __restrict__ partial) {
   double v[2] = {0.0, 0.0};
