@@ -709,22 +709,44 @@ __global__ void __launch_bounds__(THREADS, NC == 64 ? 1 : 3)
       ok = done(s, phase);
       if (!ok) break;
       acc_row<NC>(tT + ro.lane + ro.c0, v);  // (Ep U) row
-      if (ro.valid) {
-        const float2* ur = ulink + ro.m * NC + ro.c0;
-#pragma unroll
-        for (int c = 0; c < SH::HALF; c++) {
-          const float2 u = __ldg(ur + c);
-          v[c] += ro.im ? u.y : u.x;
-        }
-      }
     }
     epi_plain<NC>(s, ro, v);
     __syncthreads();
+    // U' = U + (V + g_i U_i) row by row, V = Ep U.  With reunit, g_i keeps the
+    // row's norm: g_i = -(|U_i + V_i|^2 - |U_i|^2) / (2 |U_i|^2), summed in FP32
+    // from the small terms (2 U + V) V.  The accumulation of V on the tensor
+    // cores rounds its sums toward zero (and E's projection reads E^dag E from
+    // the same accumulators), which left every row's norm off by ~1e-11 in one
+    // direction per update, an energy drift at these couplings (dH32 - dH64
+    // -0.05 to -0.08 per trajectory at SU(32) 8^4 and SU(64) 4x16^2).  The small
+    // terms are summed before the O(1) term, rounded once.
+    {
+      constexpr int TPR = THREADS / NC;  // threads per row, consecutive lanes
+      const int row = tid / TPR, sub = tid % TPR;
+      const float2* ur = ulink + (size_t)row * NC;
+      float g = 0.f;
+      if (reunit) {
+        float d = 0.f, un = 0.f;
+        for (int j = sub; j < NC; j += TPR) {
+          const float2 u = __ldg(ur + j);
+          const float vr = s.plain[row * SH::PS + j], vi = s.plain[(NC + row) * SH::PS + j];
+          d = fmaf(vr, fmaf(2.f, u.x, vr), d);
+          d = fmaf(vi, fmaf(2.f, u.y, vi), d);
+          un = fmaf(u.x, u.x, fmaf(u.y, u.y, un));
+        }
 #pragma unroll
-    for (int q = 0; q < SH::EPT; q++) {
-      const int e = tid + THREADS * q;
-      Uout[fb + 32 * (size_t)e] =
-          make_float2(s.plain[(e / NC) * SH::PS + e % NC], s.plain[(NC + e / NC) * SH::PS + e % NC]);
+        for (int o = TPR / 2; o > 0; o >>= 1) {
+          d += __shfl_xor_sync(0xffffffffu, d, o);
+          un += __shfl_xor_sync(0xffffffffu, un, o);
+        }
+        g = -0.5f * d / un;
+      }
+      for (int j = sub; j < NC; j += TPR) {
+        const float2 u = __ldg(ur + j);
+        const float wr = fmaf(g, u.x, s.plain[row * SH::PS + j]);
+        const float wi = fmaf(g, u.y, s.plain[(NC + row) * SH::PS + j]);
+        Uout[fb + 32 * (size_t)(row * NC + j)] = make_float2(u.x + wr, u.y + wi);
+      }
     }
     __syncthreads();
   }
