@@ -57,19 +57,21 @@ __device__ __forceinline__ int find_chain(const int* __restrict__ item_start, in
 }
 
 // Copies the descriptor of the chain that owns this CTA's work item into
-// shared memory; returns the item's index within its chain.
+// shared memory; returns the item's index within its chain.  Every thread
+// finds the chain (a few cached loads) and the copy is spread over the
+// threads one word each, so the CTA's start costs one round of loads instead
+// of one thread's serial copy of the whole descriptor.
 __device__ __forceinline__ int load_chain(ChainDev& sd, const ChainDev* __restrict__ descs,
                                           const int* __restrict__ item_start, const int* __restrict__ chain_ids,
                                           int nchains) {
-  __shared__ int s_local;
-  if (threadIdx.x == 0) {
-    const int k = find_chain(item_start, nchains, blockIdx.x);
-    const int c = chain_ids ? chain_ids[k] : k;
-    sd = descs[c];
-    s_local = blockIdx.x - item_start[k];
-  }
+  static_assert(sizeof(ChainDev) % 4 == 0, "descriptor copied in 4-byte words");
+  const int k = find_chain(item_start, nchains, blockIdx.x);
+  const int c = chain_ids ? __ldg(chain_ids + k) : k;
+  const uint32_t* src = reinterpret_cast<const uint32_t*>(descs + c);
+  uint32_t* dst = reinterpret_cast<uint32_t*>(&sd);
+  for (int w = threadIdx.x; w < (int)(sizeof(ChainDev) / 4); w += blockDim.x) dst[w] = __ldg(src + w);
   __syncthreads();
-  return s_local;
+  return blockIdx.x - __ldg(item_start + k);
 }
 
 // Force (+ link update) for the small-NC chains of one colour number: item =
