@@ -1114,12 +1114,11 @@ int askja_autotune(askja_ctx* c, int reps, askja_tuning* out) {
     if (dup) continue;
     seen.push_back(eff);
     cands.push_back({1, eff, 0});
-  }
-  // FP32 rows for 5 <= NC <= 8 (k_force8): tighter register budgets at the default sites per CTA
-  if (!c->split && !fp64 && c->N > 4 && c->N <= 8) {
-    const int eff = askja::rows_effective_groups(c->N, fp64, 0);
-    cands.push_back({1, eff, 1});
-    cands.push_back({1, eff, 2});
+    // FP32 rows for 5 <= NC <= 8 (k_force8): the tighter register budgets at every sites-per-CTA choice
+    if (!fp64 && c->N > 4 && c->N <= 8) {
+      cands.push_back({1, eff, 1});
+      cands.push_back({1, eff, 2});
+    }
   }
   if (cands.size() > 24) cands.resize(24);
   // scratch: Pi holds a copy of pi, the partner link buffer receives the output
