@@ -568,10 +568,11 @@ int askja_create(const askja_params* p, askja_ctx** out) {
   CKC(cudaMemset(c->tc_status, 0, sizeof(unsigned)));
   c->lc.scratch = c->staging;
   c->lc.status = c->tc_status;
-  // untuned default: tensor cores where they exist, else thread-per-link for NC <= 4
+  // untuned default: tensor cores for NC = 32 and 64, else thread-per-link for NC <= 4 (rows above);
+  // NC = 16 on the tensor cores is an explicit path and an autotuner candidate
   c->lc.force_rows = p->kernel_path != 0 ? p->kernel_path
-                     : askja::tc_supported(p->nc, p->dim, p->precision == ASKJA_FP64) ? 2
-                                                                                       : 0;
+                     : (p->nc >= 32 && askja::tc_supported(p->nc, p->dim, p->precision == ASKJA_FP64)) ? 2
+                                                                                                      : 0;
   c->lc.rows_groups = 0;
   c->lc.small_occ = 0;
   if (p->kernel_path == 0) {

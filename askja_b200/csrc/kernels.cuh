@@ -179,6 +179,7 @@ template <typename T>
 cudaError_t tc_dispatch(const LaunchCtx& c, int mode, const void* U, const void* Pin, void* Pout, void* Uout,
                         double ek, double ed) {
   if constexpr (sizeof(T) == 4) {
+    if (c.lat.N == 16) return tc_link<16>(c, mode, U, Pin, Pout, Uout, ek, ed);
     if (c.lat.N == 32) return tc_link<32>(c, mode, U, Pin, Pout, Uout, ek, ed);
     if (c.lat.N == 64) return tc_link<64>(c, mode, U, Pin, Pout, Uout, ek, ed);
   }

@@ -35,7 +35,7 @@ struct LaunchCtx {
   int rows_ns;      // row kernels, FP32: project by one Newton-Schulz step per update (the engine
                     // re-orthonormalises with the determinant phase every few trajectories)
   int force_rows;   // kernel mapping: 0 thread-per-link (NC <= 4), 1 row-per-thread,
-                    // 2 tensor cores (FP32, NC = 32 or 64, DIM >= 2), 3 site pairs in
+                    // 2 tensor cores (FP32, NC = 16, 32 or 64, DIM >= 2), 3 site pairs in
                     // packed FP32 (NC = 3, even n[DIM-1]; the fused kick+drift then
                     // expects the site-pair layout, see pair_swap)
   int rows_groups;  // row kernels: sites per CTA (0: default 128/NC)
@@ -53,7 +53,7 @@ struct LaunchCtx {
 constexpr int FULL_REUNIT_EVERY = 10;
 
 // whether the tensor-core mapping exists for this shape and precision
-inline bool tc_supported(int N, int D, bool fp64) { return !fp64 && (N == 32 || N == 64) && D >= 2; }
+inline bool tc_supported(int N, int D, bool fp64) { return !fp64 && (N == 16 || N == 32 || N == 64) && D >= 2; }
 
 // whether the site-pair mapping exists (n_fast: extent of the fastest direction)
 inline bool pair_supported(int N, int D, bool fp64, int n_fast) {

@@ -1,5 +1,5 @@
 // Tensor-core (tcgen05) link update for large colour number, FP32 storage,
-// NC = 32 and 64.  Same physics as rows::force_rows (sun.cpp:672-790,
+// NC = 16, 32 and 64.  Same physics as rows::force_rows (sun.cpp:672-790,
 // sunmat.h:200-248, 355-371): the staple sum, the traceless anti-hermitian
 // force, the momentum kick, the order-LEVEL Taylor exponential and the link
 // update, with every NC x NC complex product on the 5th-generation tensor
@@ -12,7 +12,8 @@
 // (-Xi; Xr; Xi) (3NC rows): rows NC..3NC-1 are [Xr; Xi] and rows 0..2NC-1
 // are [-Xi; Xr].  The accumulator [Cr; Ci] sits in tensor memory: row r of
 // the 2NC rows in TMEM lane r (M = 128) or lane 32(r/16) + r%16 (M = 64),
-// column c in TMEM column c.
+// column c in TMEM column c.  NC = 16 (2NC = 32 rows) issues M = 64, the
+// smallest tcgen05 shape, and ignores accumulator rows 32..63.
 //
 // Precision: split TF32 x 3 with FP32 accumulation.  Every operand x is
 // stored as hi = tf32(x) and lo = tf32(x - hi); each product takes hi*hi into
@@ -70,10 +71,26 @@ struct Shape {
   // accumulators of each at +2NC
   static constexpr int TMEM_COLS = 4 * NC;
   static constexpr uint32_t CORR = 2 * NC;
-  static constexpr int UPT = NC * NC / 4 / THREADS;  // 4-element units per thread
-  static constexpr int EPT = NC * NC / THREADS;      // elements per thread
-  static constexpr int HALF = NC / 2;                // accumulator columns per thread
+  static constexpr int UNITS = NC * NC / 4;                  // 4-element units of one matrix
+  static constexpr int UPT = (UNITS + THREADS - 1) / THREADS;  // per thread (NC = 16: a quarter of the threads)
+  static constexpr int EPT = NC * NC / THREADS;              // elements per thread
+  static constexpr int HALF = NC / 2;                        // accumulator columns per thread
+  // MMA rows: 2 NC, padded to the smallest tcgen05 shape (M = 64) for NC = 16;
+  // rows 2 NC .. 63 then read whatever follows the left operand in shared
+  // memory (the other split, the right operand) and their accumulator rows
+  // are never read
+  static constexpr int M = 2 * NC < 64 ? 64 : 2 * NC;
 };
+// the padded left-operand reads (rows from NC up to NC + M) end inside the two
+// A splits and the right operands that follow them
+static_assert(Shape<16>::A_BYTES + (16 / 8 + Shape<16>::M / 8) * Shape<16>::SBO <=
+                  2 * Shape<16>::A_BYTES + 4 * Shape<16>::B_BYTES,
+              "NC = 16 MMA reads stay in the operand region");
+// unit u of a matrix exists (always for NC >= 32)
+template <int NC>
+__device__ __forceinline__ bool unit_exists(int u) {
+  return Shape<NC>::UNITS % THREADS == 0 || u < Shape<NC>::UNITS;
+}
 
 // ---------------------------------------------------------------- PTX ----
 __device__ __forceinline__ uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -138,6 +155,19 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar) {
 
 // 32 lanes x 16 / 32 columns of 32-bit accumulator; the wait carries the
 // registers so that no use is scheduled before it
+__device__ __forceinline__ void tmem_ld(uint32_t taddr, float (&v)[8]) {
+  uint32_t r[8];
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+               : "r"(taddr)
+               : "memory");
+  asm volatile("tcgen05.wait::ld.sync.aligned;"
+               : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7])
+               :
+               : "memory");
+#pragma unroll
+  for (int i = 0; i < 8; i++) v[i] = __uint_as_float(r[i]);
+}
 __device__ __forceinline__ void tmem_ld(uint32_t taddr, float (&v)[16]) {
   uint32_t r[16];
   asm volatile(
@@ -268,6 +298,7 @@ template <int NC>
 __device__ __forceinline__ void fetch(Frag<NC>& f, const float2* __restrict__ y, bool rowkind) {
 #pragma unroll
   for (int i = 0; i < Shape<NC>::UPT; i++) {
+    if (!unit_exists<NC>(threadIdx.x + THREADS * i)) continue;
     int r, kc;
     unit_rc<NC>(threadIdx.x + THREADS * i, rowkind, r, kc);
     if (rowkind) {
@@ -295,6 +326,7 @@ __device__ __forceinline__ void put(const Smem& s, const Frag<NC>& f, int kind) 
   const bool negim = kind == A_DAG || kind == B_DAG;
 #pragma unroll
   for (int i = 0; i < Shape<NC>::UPT; i++) {
+    if (!unit_exists<NC>(threadIdx.x + THREADS * i)) continue;
     int r, kc;
     unit_rc<NC>(threadIdx.x + THREADS * i, rowkind, r, kc);
     const float4 im = negim ? neg4(f.im[i]) : f.im[i];
@@ -316,7 +348,7 @@ __device__ __forceinline__ void issue_product(const Smem& s, uint32_t dtmem, uin
   constexpr uint32_t idesc = (1u << 4)                             // D: F32
                              | (2u << 7) | (2u << 10)              // A, B: TF32
                              | ((uint32_t)(NC >> 3) << 17)         // N = NC
-                             | ((uint32_t)((2 * NC) >> 4) << 24);  // M = 2 NC
+                             | ((uint32_t)(SH::M >> 4) << 24);     // M = 2 NC (64 for NC = 16)
   // the start address is the low 14-bit field (address / 16) and every
   // operand lies below 256 KB, so offsets are added to the descriptor directly
   const uint64_t da = sdesc(saddr(s.A), LBO, SH::SBO), db = sdesc(saddr(s.B), LBO, SH::SBO);
@@ -361,11 +393,11 @@ struct Role {
       valid = true;
     } else {
       rr = 16 * q + l;
-      valid = l < 16;
+      valid = l < 16 && rr < 2 * NC;  // NC = 16: rows 32..63 are the padding of M = 64
     }
     im = rr >= NC;
     m = im ? rr - NC : rr;
-    if (!valid) {  // lanes 16..31 of each warp when M = 64: no accumulator row
+    if (!valid) {  // lanes 16..31 of each warp when M = 64, padding rows: no accumulator row
       im = false;
       m = 0;
     }
@@ -415,13 +447,21 @@ __device__ __forceinline__ void epi_B(const Smem& s, const Role<NC>& ro, const f
 // round-to-nearest addition (taddr: main accumulator + lane + column)
 template <int NC>
 __device__ __forceinline__ void acc_row(uint32_t taddr, float (&v)[Shape<NC>::HALF]) {
+  if constexpr (Shape<NC>::HALF == 8) {
+    float a[8], b[8];
+    tmem_ld(taddr, a);
+    tmem_ld(taddr + Shape<NC>::CORR, b);
 #pragma unroll
-  for (int h = 0; h < Shape<NC>::HALF; h += 16) {
-    float a[16], b[16];
-    tmem_ld(taddr + h, a);
-    tmem_ld(taddr + Shape<NC>::CORR + h, b);
+    for (int i = 0; i < 8; i++) v[i] = __fadd_rn(a[i], b[i]);
+  } else {
 #pragma unroll
-    for (int i = 0; i < 16; i++) v[h + i] = __fadd_rn(a[i], b[i]);
+    for (int h = 0; h < Shape<NC>::HALF; h += 16) {
+      float a[16], b[16];
+      tmem_ld(taddr + h, a);
+      tmem_ld(taddr + Shape<NC>::CORR + h, b);
+#pragma unroll
+      for (int i = 0; i < 16; i++) v[h + i] = __fadd_rn(a[i], b[i]);
+    }
   }
 }
 
@@ -624,6 +664,7 @@ __global__ void __launch_bounds__(THREADS, NC == 64 ? 1 : 3)
       float em[SH::HALF];
 #pragma unroll
       for (int i = 0; i < SH::UPT; i++) {  // A <- Em = i sc0 P
+        if (!unit_exists<NC>(tid + THREADS * i)) continue;
         int m, kc;
         unit_rc<NC>(tid + THREADS * i, true, m, kc);
         const float* rp = s.plain + m * SH::PS + 4 * kc;
@@ -637,6 +678,7 @@ __global__ void __launch_bounds__(THREADS, NC == 64 ? 1 : 3)
       if (order > 1) {
 #pragma unroll
         for (int i = 0; i < SH::UPT; i++) {  // B = P: Bs[j][k] = P[k][j]
+          if (!unit_exists<NC>(tid + THREADS * i)) continue;
           int j, kc;
           unit_rc<NC>(tid + THREADS * i, false, j, kc);
           const float* pr = s.plain + 4 * kc * SH::PS + j;
@@ -666,6 +708,7 @@ __global__ void __launch_bounds__(THREADS, NC == 64 ? 1 : 3)
       if (reunit) {
 #pragma unroll
         for (int i = 0; i < SH::UPT; i++) {  // A <- Em^dag, B <- Em, from columns of the plain tile
+          if (!unit_exists<NC>(tid + THREADS * i)) continue;
           int r, kc;
           unit_rc<NC>(tid + THREADS * i, false, r, kc);
           const float* pr = s.plain + 4 * kc * SH::PS + r;
@@ -689,6 +732,7 @@ __global__ void __launch_bounds__(THREADS, NC == 64 ? 1 : 3)
         epi_B<NC>(s, ro, mm);  // B <- M
 #pragma unroll
         for (int i = 0; i < SH::UPT; i++) {  // A <- Em
+          if (!unit_exists<NC>(tid + THREADS * i)) continue;
           int m, kc;
           unit_rc<NC>(tid + THREADS * i, true, m, kc);
           const float* rp = s.plain + m * SH::PS + 4 * kc;

@@ -49,6 +49,9 @@ CONFIGS = {
                    cpu_dims=[2, 2, 2, 2], ensemble=20),
     "su64_4x16": dict(nc=64, dims=[4, 16, 16], beta=8192.0, dt=0.005, level=8, nsteps=20, tensor=True,
                       cpu_dims=[2, 2, 4], ensemble=20),
+    # NC = 16: the tensor cores on the padded M = 64 shape against the row kernels (the autotuner picks)
+    "su16_6": dict(nc=16, dims=[6, 6, 6, 6], beta=512.0, dt=0.005, level=8, nsteps=20, tensor=True,
+                   cpu_dims=[2, 2, 2, 2], ensemble=20),
 }
 
 BATCH_CONFIGS = ("batch64", "batch_su3_32")
@@ -344,7 +347,7 @@ def run_ours(args):
     bytes_per_lu = link_update_bytes(nc, residual)
     achieved = alg_per_lu * links / (f32["kernel_ms"] / 1e3) / 1e9
     traffic = measured_traffic(args.config)
-    if cfg.get("tensor"):
+    if cfg.get("tensor") and (f32["tuning"]["path"] == 2 or (f32["tuning"]["path"] is None and nc >= 32)):
         fpl = tensor_flops_per_link(nc, len(dims), cfg["level"])
         sec = f32["kernel_ms"] / 1e3
         pk, src = tf32_peak()

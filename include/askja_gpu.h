@@ -76,7 +76,7 @@ typedef struct {
                           projection before every 10th trajectory */
   int device;          /* CUDA device ordinal */
   int kernel_path;     /* 0 automatic; 1 row-per-thread kernels for every NC (testing);
-                          2 tensor cores (FP32 with NC = 32 or 64 and DIM >= 2 only);
+                          2 tensor cores (FP32 with NC = 16, 32 or 64 and DIM >= 2 only);
                           3 site pairs in packed FP32 (NC = 3, FP32, DIM >= 2 and
                             an even extent N{DIM-1} only) */
   uint64_t seed;       /* Philox key for momenta, Metropolis uniforms and hot start */
@@ -225,7 +225,7 @@ ASKJA_API int askja_md_steps(askja_ctx* ctx, int nsteps, double eps);
 /* Kernel mapping for the force / link-update kernel of one (NC, DIM,
  * precision): thread-per-link (NC <= 4, all matrices in registers) or
  * row-per-thread (NC threads per link, shared-memory tiles) or tensor cores
- * (FP32, NC = 32 or 64: every complex product a split-TF32 MMA) or site pairs
+ * (FP32, NC = 16, 32 or 64: every complex product a split-TF32 MMA) or site pairs
  * (FP32 SU(3): two adjacent sites' links per thread in packed FP32x2
  * arithmetic), the number of sites per CTA of the row kernels, and the
  * register budget of the thread-per-link kernels. */

@@ -1,5 +1,6 @@
-"""Tensor-core link update (kernel_path 2: FP32 storage, NC = 32 and 64,
-every complex product a split-TF32 tcgen05 MMA) against the FP64 oracle.
+"""Tensor-core link update (kernel_path 2: FP32 storage, NC = 16, 32 and 64,
+every complex product a split-TF32 tcgen05 MMA; NC = 16 on the padded
+M = 64 shape) against the FP64 oracle.
 
 Tolerances are those of the FP32 CUDA-core path: the split keeps about 22
 mantissa bits per operand and accumulates in FP32, so force and link errors
@@ -14,7 +15,7 @@ from oracle import Oracle, fields
 
 pytestmark = pytest.mark.gpu
 
-CASES = [(32, [2, 2, 2]), (32, [3, 2]), (64, [2, 2]), (64, [2, 3, 2])]
+CASES = [(16, [2, 2, 2]), (16, [3, 2, 2]), (32, [2, 2, 2]), (32, [3, 2]), (64, [2, 2]), (64, [2, 3, 2])]
 IDS = [f"su{n}_{'x'.join(map(str, d))}" for n, d in CASES]
 
 
@@ -129,7 +130,9 @@ def test_path_validation():
     with pytest.raises(ab.AskjaError):
         ab.Engine(32, [2, 2], beta=1.0, precision="fp64", kernel_path=2)
     with pytest.raises(ab.AskjaError):
-        ab.Engine(16, [2, 2], beta=1.0, precision="fp32", kernel_path=2)
+        ab.Engine(24, [2, 2], beta=1.0, precision="fp32", kernel_path=2)
+    with pytest.raises(ab.AskjaError):
+        ab.Engine(8, [2, 2], beta=1.0, precision="fp32", kernel_path=2)
     with pytest.raises(ab.AskjaError):
         ab.Engine(32, [4], beta=1.0, precision="fp32", kernel_path=2)
     with ab.Engine(32, [2, 2], beta=1.0, precision="fp32") as e:
@@ -175,3 +178,17 @@ def test_bounded_wait_gives_up_and_context_survives():
     with ab.Engine(nc, dims, beta=2.0 * nc * nc, precision="fp32", kernel_path=1) as e:
         with pytest.raises(ab.AskjaError):
             e.tc_wait_selftest(1000)  # only on the tensor-core mapping
+
+
+def test_su16_tensor_cores_match_row_kernel_trajectory():
+    """SU(16) on the padded tensor-core shape against the FP32 row kernels and
+    the FP64 engine: one whole trajectory, same dH to 1e-3."""
+    nc, dims = 16, [2, 2, 3]
+    O, u, pi, beta = setup(nc, dims, 161)
+    res = {}
+    for path, prec in [(2, "fp32"), (1, "fp32"), (0, "fp64")]:
+        with ab.Engine(nc, dims, beta=beta, dt=0.005, level=8, precision=prec, kernel_path=path, seed=7) as e:
+            e.set_links(u)
+            res[path] = e.trajectory(10)
+    assert abs(res[2]["dh"] - res[0]["dh"]) < 1e-3
+    assert abs(res[1]["dh"] - res[0]["dh"]) < 1e-3
