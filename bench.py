@@ -439,7 +439,7 @@ def run_ours(args):
         "clocks": f32["clocks"],
     }
     if args.config == "su3_32" and not args.no_batch:
-        # the north-star path: FP32-mixed chains batched in one engine vs each chain alone in FP64
+        # the batched path: FP32-mixed chains batched in one engine vs each chain alone in FP64
         b = run_batch(argparse.Namespace(config="batch_su3_32", steps=max(3, args.steps // 2), warmup=args.warmup,
                                          therm=args.batch_therm))
         line["batched"] = {k: b[k] for k in ("metric", "value", "unit", "steps", "ms_per_step", "alone_fp64",
