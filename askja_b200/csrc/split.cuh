@@ -246,6 +246,19 @@ __device__ __forceinline__ void load_exact(small::Mat<N, double>& M, const float
     }
 }
 
+// row i of link (d, s) as hi + lo in FP64
+template <int N>
+__device__ __forceinline__ void load_exact_row(cpx<double> (&r)[N], const float2* __restrict__ U,
+                                               const uint32_t* __restrict__ UL, const Lat& L, int d, int s, int i) {
+  const size_t b = mbase(L, d, s) + (size_t)i * N * 32;
+#pragma unroll
+  for (int j = 0; j < N; j++) {
+    const float2 h = U[b + j * 32];
+    const uint32_t w = UL[b + j * 32];
+    r[j] = mkc<double>((double)h.x + (double)lo_low(w), (double)h.y + (double)lo_high(w));
+  }
+}
+
 template <int N>
 __device__ __forceinline__ void store_exact(float2* __restrict__ U, uint32_t* __restrict__ UL,
                                             const small::Mat<N, double>& M, const Lat& L, int d, int s) {
@@ -553,38 +566,42 @@ __device__ __forceinline__ void plaq_site(const Lat& L, const float2* __restrict
   if (s < L.V && counted(L, s)) {
     for (int mu = 0; mu < L.D; mu++) {
       const int xpmu = nb_plus(L, mu, s);
-      small::Mat<N, double> A, B;
-      load_exact<N>(A, U, UL, L, mu, s);
       for (int nu = mu + 1; nu < L.D; nu++) {
         const int xpnu = nb_plus(L, nu, s);
-        small::Mat<N, double> C, Dn;
+        // B and C whole, A = U_mu(s) and Dn = U_nu(s) a row at a time (the
+        // products and sums in the same order as with all four matrices held)
+        small::Mat<N, double> B, C;
         load_exact<N>(B, U, UL, L, nu, xpmu);
         load_exact<N>(C, U, UL, L, mu, xpnu);
-        load_exact<N>(Dn, U, UL, L, nu, s);
         double tr = 0.0;
 #pragma unroll
-        for (int i = 0; i < N; i++)
+        for (int i = 0; i < N; i++) {
+          cpx<double> a[N], dn[N];
+          load_exact_row<N>(a, U, UL, L, mu, s, i);
+          load_exact_row<N>(dn, U, UL, L, nu, s, i);
 #pragma unroll
           for (int j = 0; j < N; j++) {
             cpx<double> ab = czero<double>(), dc = czero<double>();
 #pragma unroll
             for (int k = 0; k < N; k++) {
-              cmac(ab, A.a[i][k], B.a[k][j]);
-              cmac(dc, Dn.a[i][k], C.a[k][j]);
+              cmac(ab, a[k], B.a[k][j]);
+              cmac(dc, dn[k], C.a[k][j]);
             }
             tr = fma(ab.re, dc.re, tr);
             tr = fma(ab.im, dc.im, tr);
           }
+        }
         v[mu == 0 ? 0 : 1] += 1.0 - tr / N;
       }
     }
   }
 }
 
-// At most 128 registers (two 256-thread CTAs per SM): unbounded, the four FP64
-// matrices took 172 and left one CTA per SM.
+// N <= 3: at most 128 registers (two 256-thread CTAs per SM; with all four
+// matrices held, unbounded, it took 172 and left one).  N = 4 keeps its two whole
+// FP64 matrices in registers (one CTA per SM; capped at 128 it spills 1.5 KB).
 template <int N>
-__global__ void __launch_bounds__(misc::RED_THREADS, 2) k_plaq(Lat L, const float2* __restrict__ U,
+__global__ void __launch_bounds__(misc::RED_THREADS, N <= 3 ? 2 : 1) k_plaq(Lat L, const float2* __restrict__ U,
                                                             const uint32_t* __restrict__ UL,
                                                             double* __restrict__ partial) {
   double v[2] = {0.0, 0.0};
