@@ -536,8 +536,13 @@ __device__ __forceinline__ Term staple_term(const Lat& L, const float2* __restri
 // MODE 1: also Uout = exp(i eps_d Pout) U (reunitarised when reunit)
 // MODE 2: Uout = exp(i eps_d Pin) U only
 // U is read from `aos` (per-link contiguous copy); Uout may be U itself.
+// Register budget: NC = 64 one CTA per SM (its shared memory allows no
+// second); NC = 16 and 32 at most 64 registers, four CTAs per SM, whose
+// products and epilogues overlap (SU(32) 8^4 2.31 -> 2.23 ms, SU(16) 6^4
+// 0.352 -> 0.301 ms per fused step against three CTAs; five: no faster, six
+// spill).
 template <int NC, int MODE>
-__global__ void __launch_bounds__(THREADS, NC == 64 ? 1 : 3)
+__global__ void __launch_bounds__(THREADS, NC == 64 ? 1 : 4)
     k_link(Lat L, const float2* __restrict__ aos, const float2* Pin, float2* Pout, float2* Uout, float eps_k,
            float eps_d, int order, int reunit, unsigned* status) {
   using SH = Shape<NC>;
