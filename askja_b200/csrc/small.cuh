@@ -53,9 +53,47 @@ __device__ __forceinline__ void zero(Mat<N, T>& m) {
     for (int j = 0; j < N; j++) m.a[i][j] = czero<T>();
 }
 
+// Row i of A times B^dag added to (re, im) pairs in packed FP32x2: per
+// element the multiply-adds of cmac_nc in the same order (re: a.re b.re then
+// a.im b.im; im: a.im b.re then -a.re b.im), two FFMA2 instead of four FFMA,
+// so the results are bit-identical.  A's (re, im) pair is used as loaded and
+// needs one swapped, negated copy per element, B's parts are broadcast.  Only
+// the A B^dag products are packed: the same form for A B and A^dag B^dag needs
+// a swapped or negated copy of every element of the right operand and made
+// the FP32 SU(3) kernels slower (residual planes 395 -> 402-405 us per launch
+// at 32^4; FP32-only storage 363 -> 361-370 us).
+template <int N>
+__device__ __forceinline__ void row_nd_x2(float2 (&c)[N], const Mat<N, float>& A, const Mat<N, float>& B, int i) {
+  float2 an[N], ar[N];
+#pragma unroll
+  for (int k = 0; k < N; k++) {
+    an[k] = make_float2(A.a[i][k].re, A.a[i][k].im);
+    ar[k] = make_float2(A.a[i][k].im, -A.a[i][k].re);
+  }
+#pragma unroll
+  for (int j = 0; j < N; j++)
+#pragma unroll
+    for (int k = 0; k < N; k++) {
+      c[j] = __ffma2_rn(an[k], make_float2(B.a[j][k].re, B.a[j][k].re), c[j]);
+      c[j] = __ffma2_rn(ar[k], make_float2(B.a[j][k].im, B.a[j][k].im), c[j]);
+    }
+}
+
 // C = A * B^dag (rows 0 .. ROWS-1)
 template <int N, typename T, int ROWS = N>
 __device__ __forceinline__ void mul_nd(Mat<N, T>& C, const Mat<N, T>& A, const Mat<N, T>& B) {
+  if constexpr (sizeof(T) == 4) {
+#pragma unroll
+    for (int i = 0; i < ROWS; i++) {
+      float2 c[N];
+#pragma unroll
+      for (int j = 0; j < N; j++) c[j] = make_float2(0.f, 0.f);
+      row_nd_x2<N>(c, A, B, i);
+#pragma unroll
+      for (int j = 0; j < N; j++) C.a[i][j] = mkc<T>(c[j].x, c[j].y);
+    }
+    return;
+  }
 #pragma unroll
   for (int i = 0; i < ROWS; i++)
 #pragma unroll
@@ -69,6 +107,18 @@ __device__ __forceinline__ void mul_nd(Mat<N, T>& C, const Mat<N, T>& A, const M
 // C += A * B^dag
 template <int N, typename T>
 __device__ __forceinline__ void mac_nd(Mat<N, T>& C, const Mat<N, T>& A, const Mat<N, T>& B) {
+  if constexpr (sizeof(T) == 4) {
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+      float2 c[N];
+#pragma unroll
+      for (int j = 0; j < N; j++) c[j] = make_float2(C.a[i][j].re, C.a[i][j].im);
+      row_nd_x2<N>(c, A, B, i);
+#pragma unroll
+      for (int j = 0; j < N; j++) C.a[i][j] = mkc<T>(c[j].x, c[j].y);
+    }
+    return;
+  }
 #pragma unroll
   for (int i = 0; i < N; i++)
 #pragma unroll
