@@ -53,114 +53,133 @@ __device__ __forceinline__ void zero(Mat<N, T>& m) {
     for (int j = 0; j < N; j++) m.a[i][j] = czero<T>();
 }
 
-// Row i of A times B^dag added to (re, im) pairs in packed FP32x2: per
-// element the multiply-adds of cmac_nc in the same order (re: a.re b.re then
-// a.im b.im; im: a.im b.re then -a.re b.im), two FFMA2 instead of four FFMA,
-// so the results are bit-identical.  A's (re, im) pair is used as loaded and
-// needs one swapped, negated copy per element, B's parts are broadcast.  Only
-// the A B^dag products are packed: the same form for A B and A^dag B^dag needs
-// a swapped or negated copy of every element of the right operand and made
-// the FP32 SU(3) kernels slower (residual planes 395 -> 402-405 us per launch
-// at 32^4; FP32-only storage 363 -> 361-370 us).
-template <int N>
-__device__ __forceinline__ void row_nd_x2(float2 (&c)[N], const Mat<N, float>& A, const Mat<N, float>& B, int i) {
+// FP32 products in packed FP32x2 (FFMA2 of sm_100).  Every product is
+// written as X Y^dag: for each element, (re, im) += (x.re, x.im) * (y.re, y.re)
+// then += (x.im, -x.re) * (y.im, y.im), two FFMA2 per complex multiply-add
+// instead of four FFMA; the left element is used as loaded plus one swapped,
+// negated copy, the right one's parts are broadcast (negated where Y is a
+// conjugate).  A B is A (B^dag)^dag, A^dag B^dag is (A^dag) B^dag.  Per
+// element A B^dag adds its terms in the order of cmac_nc (bit-identical to
+// the scalar form); A B and A^dag B^dag add the imaginary part's two terms in
+// the other order than cmac / cmac_cc.  At SU(3) 32^4 this took the residual-plane fused kernel
+// from 409 to 388 us and the FP32-only one from 385 to 349 us (A B with
+// broadcast left parts and a swapped right copy instead: 402-405 us).
+// c[j] += sum_k x(k) conj(y(j, k)) for the N columns j of one row
+template <int N, typename FL, typename FR>
+__device__ __forceinline__ void row_x2(float2 (&c)[N], FL&& x, FR&& y) {
   float2 an[N], ar[N];
 #pragma unroll
   for (int k = 0; k < N; k++) {
-    an[k] = make_float2(A.a[i][k].re, A.a[i][k].im);
-    ar[k] = make_float2(A.a[i][k].im, -A.a[i][k].re);
+    const cpx<float> a = x(k);
+    an[k] = make_float2(a.re, a.im);
+    ar[k] = make_float2(a.im, -a.re);
   }
 #pragma unroll
   for (int j = 0; j < N; j++)
 #pragma unroll
     for (int k = 0; k < N; k++) {
-      c[j] = __ffma2_rn(an[k], make_float2(B.a[j][k].re, B.a[j][k].re), c[j]);
-      c[j] = __ffma2_rn(ar[k], make_float2(B.a[j][k].im, B.a[j][k].im), c[j]);
+      const cpx<float> b = y(j, k);
+      c[j] = __ffma2_rn(an[k], make_float2(b.re, b.re), c[j]);
+      c[j] = __ffma2_rn(ar[k], make_float2(b.im, b.im), c[j]);
     }
+}
+
+// rows 0 .. ROWS-1 of C (+)= X Y^dag in FP32, X and Y given element-wise
+template <int N, int ROWS, bool ACC, typename FL, typename FR>
+__device__ __forceinline__ void prod_x2(Mat<N, float>& C, FL&& x, FR&& y) {
+#pragma unroll
+  for (int i = 0; i < ROWS; i++) {
+    float2 c[N];
+#pragma unroll
+    for (int j = 0; j < N; j++) c[j] = ACC ? make_float2(C.a[i][j].re, C.a[i][j].im) : make_float2(0.f, 0.f);
+    row_x2<N>(c, [&](int k) { return x(i, k); }, y);
+#pragma unroll
+    for (int j = 0; j < N; j++) C.a[i][j] = mkc<float>(c[j].x, c[j].y);
+  }
 }
 
 // C = A * B^dag (rows 0 .. ROWS-1)
 template <int N, typename T, int ROWS = N>
 __device__ __forceinline__ void mul_nd(Mat<N, T>& C, const Mat<N, T>& A, const Mat<N, T>& B) {
   if constexpr (sizeof(T) == 4) {
+    prod_x2<N, ROWS, false>(C, [&](int i, int k) { return A.a[i][k]; }, [&](int j, int k) { return B.a[j][k]; });
+  } else {
 #pragma unroll
-    for (int i = 0; i < ROWS; i++) {
-      float2 c[N];
+    for (int i = 0; i < ROWS; i++)
 #pragma unroll
-      for (int j = 0; j < N; j++) c[j] = make_float2(0.f, 0.f);
-      row_nd_x2<N>(c, A, B, i);
+      for (int j = 0; j < N; j++) {
+        cpx<T> s = czero<T>();
 #pragma unroll
-      for (int j = 0; j < N; j++) C.a[i][j] = mkc<T>(c[j].x, c[j].y);
-    }
-    return;
+        for (int k = 0; k < N; k++) cmac_nc(s, A.a[i][k], B.a[j][k]);
+        C.a[i][j] = s;
+      }
   }
-#pragma unroll
-  for (int i = 0; i < ROWS; i++)
-#pragma unroll
-    for (int j = 0; j < N; j++) {
-      cpx<T> s = czero<T>();
-#pragma unroll
-      for (int k = 0; k < N; k++) cmac_nc(s, A.a[i][k], B.a[j][k]);
-      C.a[i][j] = s;
-    }
 }
 // C += A * B^dag
 template <int N, typename T>
 __device__ __forceinline__ void mac_nd(Mat<N, T>& C, const Mat<N, T>& A, const Mat<N, T>& B) {
   if constexpr (sizeof(T) == 4) {
+    prod_x2<N, N, true>(C, [&](int i, int k) { return A.a[i][k]; }, [&](int j, int k) { return B.a[j][k]; });
+  } else {
 #pragma unroll
-    for (int i = 0; i < N; i++) {
-      float2 c[N];
+    for (int i = 0; i < N; i++)
 #pragma unroll
-      for (int j = 0; j < N; j++) c[j] = make_float2(C.a[i][j].re, C.a[i][j].im);
-      row_nd_x2<N>(c, A, B, i);
+      for (int j = 0; j < N; j++)
 #pragma unroll
-      for (int j = 0; j < N; j++) C.a[i][j] = mkc<T>(c[j].x, c[j].y);
-    }
-    return;
+        for (int k = 0; k < N; k++) cmac_nc(C.a[i][j], A.a[i][k], B.a[j][k]);
   }
-#pragma unroll
-  for (int i = 0; i < N; i++)
-#pragma unroll
-    for (int j = 0; j < N; j++)
-#pragma unroll
-      for (int k = 0; k < N; k++) cmac_nc(C.a[i][j], A.a[i][k], B.a[j][k]);
 }
 // C = A^dag * B^dag  (= (B A)^dag; rows 0 .. ROWS-1)
 template <int N, typename T, int ROWS = N>
 __device__ __forceinline__ void mul_dd(Mat<N, T>& C, const Mat<N, T>& A, const Mat<N, T>& B) {
+  if constexpr (sizeof(T) == 4) {
+    prod_x2<N, ROWS, false>(
+        C, [&](int i, int k) { return mkc<float>(A.a[k][i].re, -A.a[k][i].im); },
+        [&](int j, int k) { return B.a[j][k]; });
+  } else {
 #pragma unroll
-  for (int i = 0; i < ROWS; i++)
+    for (int i = 0; i < ROWS; i++)
 #pragma unroll
-    for (int j = 0; j < N; j++) {
-      cpx<T> s = czero<T>();
+      for (int j = 0; j < N; j++) {
+        cpx<T> s = czero<T>();
 #pragma unroll
-      for (int k = 0; k < N; k++) cmac_cc(s, A.a[k][i], B.a[j][k]);
-      C.a[i][j] = s;
-    }
+        for (int k = 0; k < N; k++) cmac_cc(s, A.a[k][i], B.a[j][k]);
+        C.a[i][j] = s;
+      }
+  }
 }
 // C += A * B
 template <int N, typename T>
 __device__ __forceinline__ void mac_nn(Mat<N, T>& C, const Mat<N, T>& A, const Mat<N, T>& B) {
+  if constexpr (sizeof(T) == 4) {
+    prod_x2<N, N, true>(C, [&](int i, int k) { return A.a[i][k]; },
+                        [&](int j, int k) { return mkc<float>(B.a[k][j].re, -B.a[k][j].im); });
+  } else {
 #pragma unroll
-  for (int i = 0; i < N; i++)
+    for (int i = 0; i < N; i++)
 #pragma unroll
-    for (int j = 0; j < N; j++)
+      for (int j = 0; j < N; j++)
 #pragma unroll
-      for (int k = 0; k < N; k++) cmac(C.a[i][j], A.a[i][k], B.a[k][j]);
+        for (int k = 0; k < N; k++) cmac(C.a[i][j], A.a[i][k], B.a[k][j]);
+  }
 }
 // C = A * B
 template <int N, typename T>
 __device__ __forceinline__ void mul_nn(Mat<N, T>& C, const Mat<N, T>& A, const Mat<N, T>& B) {
+  if constexpr (sizeof(T) == 4) {
+    prod_x2<N, N, false>(C, [&](int i, int k) { return A.a[i][k]; },
+                         [&](int j, int k) { return mkc<float>(B.a[k][j].re, -B.a[k][j].im); });
+  } else {
 #pragma unroll
-  for (int i = 0; i < N; i++)
+    for (int i = 0; i < N; i++)
 #pragma unroll
-    for (int j = 0; j < N; j++) {
-      cpx<T> s = czero<T>();
+      for (int j = 0; j < N; j++) {
+        cpx<T> s = czero<T>();
 #pragma unroll
-      for (int k = 0; k < N; k++) cmac(s, A.a[i][k], B.a[k][j]);
-      C.a[i][j] = s;
-    }
+        for (int k = 0; k < N; k++) cmac(s, A.a[i][k], B.a[k][j]);
+        C.a[i][j] = s;
+      }
+  }
 }
 
 // Third row of an SU(3) matrix from the first two: conj(r0 x r1).
