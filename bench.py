@@ -743,8 +743,8 @@ def run_kernel_only(args):
     nc, dims = cfg["nc"], cfg["dims"]
     with ab.Engine(nc, dims, beta=cfg["beta"], dt=cfg["dt"], level=cfg["level"], precision=args.precision,
                    kernel_path=args.path) as e:
-        if args.occ:
-            ab.set_tuning(e, {"path": args.path, "occupancy": args.occ})
+        if args.occ or args.groups:
+            ab.set_tuning(e, {"path": args.path, "occupancy": args.occ, "groups": args.groups})
         e.hot_start(11)
         e.initializeE(11, 0)
         for _ in range(args.warmup):
@@ -752,6 +752,7 @@ def run_kernel_only(args):
         e.sync()
         ms = time_fused_kernel(e, e.stream_ptr, 0, args.steps, cfg["dt"])
     return {"kernel_only": args.config, "precision": args.precision, "path": args.path, "occ": args.occ,
+            "groups": args.groups,
             "launches": 3 * args.steps + 2, "avg_launch_ms": ms,
             "link_updates_per_s": int(np.prod(dims)) * len(dims) / (ms / 1e3)}
 
@@ -774,6 +775,7 @@ def main():
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp32-lean", "fp64"], help="with --kernel-only")
     ap.add_argument("--path", type=int, default=0, help="with --kernel-only: askja kernel_path")
     ap.add_argument("--occ", type=int, default=0, help="with --kernel-only: register budget (askja_tuning.occupancy)")
+    ap.add_argument("--groups", type=int, default=0, help="with --kernel-only: askja_tuning.groups")
     args = ap.parse_args()
     if args.kernel_only:
         line = run_kernel_only(args)
