@@ -47,6 +47,7 @@ struct askja_batch {
     std::vector<int> chains;
     int* d_start = nullptr;
     int* d_ids = nullptr;
+    int* d_item = nullptr;  // small path: per item, chain index (into the descriptors) and tile, interleaved
     int nitems = 0;
   };
   std::vector<Group> groups;
@@ -127,9 +128,9 @@ cudaError_t launch_force(askja_batch* b, const askja_batch::Group& g, cudaStream
 #define SPLIT(NN)                                                                                                \
   if (g.N == NN) {                                                                                               \
     if (mode)                                                                                                    \
-      kb_force_split<NN, 1><<<grid, blk, 0, st>>>(b->d_desc, g.d_start, g.d_ids, (int)g.chains.size(), b->cur, ks); \
+      kb_force_split<NN, 1><<<grid, blk, 0, st>>>(b->d_desc, (const int2*)g.d_item, b->cur, ks);                 \
     else                                                                                                         \
-      kb_force_split<NN, 0><<<grid, blk, 0, st>>>(b->d_desc, g.d_start, g.d_ids, (int)g.chains.size(), b->cur, ks); \
+      kb_force_split<NN, 0><<<grid, blk, 0, st>>>(b->d_desc, (const int2*)g.d_item, b->cur, ks);                 \
     return cudaGetLastError();                                                                                   \
   }
       SPLIT(2) SPLIT(3) SPLIT(4)
@@ -403,9 +404,16 @@ int askja_batch_create(const askja_chain_params* chains, int nchains, int precis
     g.chains = kv.second;
     const int N = kv.first;
     std::vector<int> start(1, 0);
+    std::vector<int> item;
     if (N <= 4) {
       g.N = N;
-      for (int c : g.chains) start.push_back(start.back() + b->desc[c].lat.B);
+      for (int c : g.chains) {
+        start.push_back(start.back() + b->desc[c].lat.B);
+        for (int t = 0; t < b->desc[c].lat.B; t++) {
+          item.push_back(c);
+          item.push_back(t);
+        }
+      }
     } else {
       g.N = 0;
       g.nmax = N <= 8 ? 8 : N <= 16 ? 16 : N <= 32 ? 32 : 64;
@@ -421,6 +429,8 @@ int askja_batch_create(const askja_chain_params* chains, int nchains, int precis
     g.nitems = start.back();
     if (int rc = upload_ints(b, &g.d_start, start)) return fail(rc);
     if (int rc = upload_ints(b, &g.d_ids, g.chains)) return fail(rc);
+    if (!item.empty())
+      if (int rc = upload_ints(b, &g.d_item, item)) return fail(rc);
     b->groups.push_back(g);
   }
   b->side.resize(b->groups.size());

@@ -100,36 +100,38 @@ __device__ __forceinline__ void force_small_item(const ChainDev* __restrict__ de
     small::force_link<N, T, S2, MODE>(L, U, P, P, Uo, ek, ed, order, reunit, mu, x);
 }
 
-// The residual-plane kernel on the same tiles (split::link_update).
+// The residual-plane kernel on the same tiles (split::link_update).  The CTA
+// finds its chain and tile in one load from the per-item table (chain, tile)
+// and every thread reads the descriptor fields it uses straight from global
+// memory (the same few cache lines for the whole CTA): two dependent loads
+// before the first link load, where a binary search over the chain starts, a
+// descriptor copy to shared memory and a barrier took several.
 template <int N, int MODE>
 __device__ __forceinline__ void force_split_item(const ChainDev* __restrict__ descs,
-                                                 const int* __restrict__ item_start,
-                                                 const int* __restrict__ chain_ids, int nchains, int cur,
-                                                 double kick_scale) {
-  __shared__ ChainDev sd;
-  const int tile = load_chain(sd, descs, item_start, chain_ids, nchains);
-  const Lat L = sd.lat;
-  const int x = tile * 32 + (threadIdx.x & 31);
+                                                 const int2* __restrict__ item_chain, int cur, double kick_scale) {
+  const int2 ct = __ldg(item_chain + blockIdx.x);
+  const ChainDev* __restrict__ d = descs + ct.x;
+  const Lat L = d->lat;
+  const int x = ct.y * 32 + (threadIdx.x & 31);
   if (x >= L.V) return;
-  const float2* U = (const float2*)sd.U[cur];
-  const uint32_t* UL = (const uint32_t*)sd.UL[cur];
-  float* P = (float*)sd.PC;
-  uint32_t* PL = (uint32_t*)sd.PCL;
-  float2* Uo = (float2*)sd.U[cur ^ 1];
-  uint32_t* ULo = (uint32_t*)sd.UL[cur ^ 1];
-  const float ek = (float)(kick_scale * sd.dt), ed = (float)sd.dt;
-  const int order = sd.order;
+  const float2* U = (const float2*)d->U[cur];
+  const uint32_t* UL = (const uint32_t*)d->UL[cur];
+  float* P = (float*)d->PC;
+  uint32_t* PL = (uint32_t*)d->PCL;
+  float2* Uo = (float2*)d->U[cur ^ 1];
+  uint32_t* ULo = (uint32_t*)d->UL[cur ^ 1];
+  const float ek = (float)(kick_scale * d->dt), ed = (float)d->dt;
+  const int order = d->order;
   for (int mu = threadIdx.x >> 5; mu < L.D; mu += (blockDim.x >> 5))
     split::link_update<N, MODE>(L, U, UL, P, PL, P, PL, Uo, ULo, ek, ed, order, mu, x);
 }
 
 // SU(3): seven resident CTAs per SM, as the single-chain kernel's tuned budget
 template <int N, int MODE>
-__global__ void __launch_bounds__(128, N == 3 ? 7 : 1) kb_force_split(const ChainDev* __restrict__ descs,
-                                                                       const int* __restrict__ item_start,
-                                                                       const int* __restrict__ chain_ids,
-                                                                       int nchains, int cur, double kick_scale) {
-  force_split_item<N, MODE>(descs, item_start, chain_ids, nchains, cur, kick_scale);
+__global__ void __launch_bounds__(128, N == 3 ? 7 : 4) kb_force_split(const ChainDev* __restrict__ descs,
+                                                                       const int2* __restrict__ item_chain, int cur,
+                                                                       double kick_scale) {
+  force_split_item<N, MODE>(descs, item_chain, cur, kick_scale);
 }
 
 template <int N, typename T, int MODE>
