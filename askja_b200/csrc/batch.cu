@@ -47,7 +47,7 @@ struct askja_batch {
     std::vector<int> chains;
     int* d_start = nullptr;
     int* d_ids = nullptr;
-    int* d_item = nullptr;  // small path: per item, chain index (into the descriptors) and tile, interleaved
+    int* d_item = nullptr;  // per item: chain index (into the descriptors) and item within the chain, interleaved
     int nitems = 0;
   };
   std::vector<Group> groups;
@@ -165,7 +165,7 @@ cudaError_t launch_force(askja_batch* b, const askja_batch::Group& g, cudaStream
     if constexpr (sizeof(T) == 4 && NM == 8)                                                                  \
       if (mode) k = kb_force_rows8f;                                                                          \
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.smem);                        \
-    k<<<grid, blk, g.smem, st>>>(b->d_desc, g.d_start, g.d_ids, (int)g.chains.size(), b->cur, ks);          \
+    k<<<grid, blk, g.smem, st>>>(b->d_desc, (const int2*)g.d_item, b->cur, ks);                              \
   }
   ROWS(8) ROWS(16) ROWS(32) ROWS(64)
 #undef ROWS
@@ -423,7 +423,12 @@ int askja_batch_create(const askja_chain_params* chains, int nchains, int precis
         askja::detail::Rows<float>::shape(N, &g.G, &g.smem);
       for (int c : g.chains) {
         const Lat& L = b->desc[c].lat;
-        start.push_back(start.back() + (int)((L.V + g.G - 1) / g.G) * L.D);
+        const int n = (int)((L.V + g.G - 1) / g.G) * L.D;
+        start.push_back(start.back() + n);
+        for (int t = 0; t < n; t++) {
+          item.push_back(c);
+          item.push_back(t);
+        }
       }
     }
     g.nitems = start.back();

@@ -74,6 +74,20 @@ __device__ __forceinline__ int load_chain(ChainDev& sd, const ChainDev* __restri
   return blockIdx.x - __ldg(item_start + k);
 }
 
+// Copies the descriptor of the chain named by this CTA's entry (chain, item)
+// of the per-item table into shared memory; returns the item's index within
+// its chain (one load instead of load_chain's binary search).
+__device__ __forceinline__ int load_chain_at(ChainDev& sd, const ChainDev* __restrict__ descs,
+                                             const int2* __restrict__ item_chain) {
+  static_assert(sizeof(ChainDev) % 4 == 0, "descriptor copied in 4-byte words");
+  const int2 ct = __ldg(item_chain + blockIdx.x);
+  const uint32_t* src = reinterpret_cast<const uint32_t*>(descs + ct.x);
+  uint32_t* dst = reinterpret_cast<uint32_t*>(&sd);
+  for (int w = threadIdx.x; w < (int)(sizeof(ChainDev) / 4); w += blockDim.x) dst[w] = __ldg(src + w);
+  __syncthreads();
+  return ct.y;
+}
+
 // Force (+ link update) for the small-NC chains of one colour number: item =
 // 32-site tile, 32*min(D,4) threads (see small::k_force).
 // BYVAL: the geometry by value, so that the fields the force uses (V, B, D,
@@ -154,14 +168,14 @@ __global__ void __launch_bounds__(128, 7) kb_force_small3f(const ChainDev* __res
 // Same for the row-per-thread path: item = G consecutive sites of one
 // direction (G = blockDim / NC), directions of a site block adjacent.
 template <int NMAX, typename T, int MODE>
-__global__ void kb_force_rows(const ChainDev* __restrict__ descs, const int* __restrict__ item_start,
-                              const int* __restrict__ chain_ids, int nchains, int cur, double kick_scale) {
+__global__ void kb_force_rows(const ChainDev* __restrict__ descs, const int2* __restrict__ item_chain, int cur,
+                              double kick_scale) {
   using S2 = typename Storage<T>::type;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int piv_s[64];
   __shared__ cpx<T> det_s[64];
   __shared__ ChainDev sd;
-  const int item = load_chain(sd, descs, item_start, chain_ids, nchains);
+  const int item = load_chain_at(sd, descs, item_chain);
   const int G = blockDim.x / sd.lat.N;
   rows::force_rows<NMAX, T, S2, MODE>(sd.lat, (const S2*)sd.U[cur], (const S2*)sd.P, (S2*)sd.P,
                                       (S2*)sd.U[cur ^ 1], (T)(kick_scale * sd.dt), (T)sd.dt, sd.order, sd.reunit,
@@ -171,14 +185,13 @@ __global__ void kb_force_rows(const ChainDev* __restrict__ descs, const int* __r
 // FP32 with NMAX = 8, fused kick + drift: at most 128 registers (four
 // 128-thread CTAs per SM), as the single-chain rows::k_force8.
 static __global__ void __launch_bounds__(256, 2) kb_force_rows8f(const ChainDev* __restrict__ descs,
-                                                          const int* __restrict__ item_start,
-                                                          const int* __restrict__ chain_ids, int nchains, int cur,
+                                                          const int2* __restrict__ item_chain, int cur,
                                                           double kick_scale) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int piv_s[64];
   __shared__ cpx<float> det_s[64];
   __shared__ ChainDev sd;
-  const int item = load_chain(sd, descs, item_start, chain_ids, nchains);
+  const int item = load_chain_at(sd, descs, item_chain);
   const int G = blockDim.x / sd.lat.N;
   rows::force_rows<8, float, float2, 1>(sd.lat, (const float2*)sd.U[cur], (const float2*)sd.P, (float2*)sd.P,
                                         (float2*)sd.U[cur ^ 1], (float)(kick_scale * sd.dt), (float)sd.dt, sd.order,
