@@ -1,10 +1,12 @@
 // Kernels that advance many independent Markov chains of uneven shape (NC,
 // DIM, extents, BETA, DT) together.  Every launch covers all chains (of one
 // colour number for the force) through a work list: work item i belongs to
-// the chain c with item_start[c] <= i < item_start[c+1]; the CTA copies that
-// chain's descriptor into shared memory and runs the same per-link / per-site
-// code as the single-chain kernels (small.cuh, rows.cuh, misc.cuh).  Chains
-// of different sizes therefore share the GPU in proportion to their work.
+// the chain c with item_start[c] <= i < item_start[c+1] (the force launches,
+// which run every MD step, read (chain, item within the chain) from a per-item
+// table instead); the CTA takes that chain's descriptor and runs the same
+// per-link / per-site code as the single-chain kernels (small.cuh, rows.cuh,
+// split.cuh, misc.cuh).  Chains of different sizes therefore share the GPU in
+// proportion to their work.
 #pragma once
 
 #include <type_traits>
